@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the fused viscoelastic time step (one JSON line on rank 0).
+
+A bench "step" is one whole forward solve of the single-shot workload:
+2048 x 1024 grid, dx = 5 m, dt = 0.4 ms, 4000 time steps, FP32, seeded
+8-layer VTI medium with 3 SLS mechanisms, 40-cell CPML, free surface,
+12 Hz explosive Ricker and 512 receivers (synthetic inputs).
+
+  value  Gpt/s = nx*nz*nt / time, inputs resident in HBM, max over ranks,
+         summed over ranks (one independent shot per GPU: weak scaling)
+  e2e    the same through vi_forward_host with pinned host buffers: medium
+         and wavelet upload, the solve, and the trace download per step
+  roofline  algorithmic bytes per fused launch / mean launch time vs the
+         measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (FP32 twin, all host threads) on a bounded
+         sample of the same workload (rank 0, N = 1)
+
+`--impl reference` times the reference's CPU path instead: the reference is
+Julia (absent here) and its step does not execute, so the CPU restatement
+in oracle/ stands in for it, on all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gpt/s & % HBM roofline per step; shots/s + p50/p99 latency, batched vs plain @1e-5"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nx", type=int, default=2048)
+    p.add_argument("--nz", type=int, default=1024)
+    p.add_argument("--nt", type=int, default=4000)
+    p.add_argument("--kind", default="vti", choices=["iso", "vti", "tti"])
+    p.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    p.add_argument("--variant", type=int, default=0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def workload(a):
+    from viscoelasticinversion_b200 import media
+
+    return media.layered(nx=a.nx, nz=a.nz, nt=a.nt, kind=a.kind, seed=0)
+
+
+def workload_name(a):
+    return f"{a.kind}-layered-{a.nx}x{a.nz}-nt{a.nt}-{a.precision}-3sls-cpml40-freesurface"
+
+
+class Clocks:
+    """nvidia-smi sampling of this GPU's clocks during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str):
+        self.uuid = uuid
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines()]
+        os.unlink(self.f.name)
+        mine = [r for r in rows if len(r) >= 8 and (not self.uuid or r[0].strip().endswith(self.uuid))]
+        if not mine:
+            mine = [r for r in rows if len(r) >= 8]
+        sm = [float(r[1]) for r in mine if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in mine if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in mine for k in range(4) if "Active" == r[4 + k].strip()})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(mine)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs"), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name: str):
+    """DRAM bytes per launch of the fused kernel from the committed ncu
+    summary of this workload (profiles/), or None."""
+    f = ROOT / "profiles" / f"{name}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1].split()[0])
+    return None
+
+
+def cpu_baseline(w, seconds: float):
+    """Times the FP32 CPU oracle on the first steps of the workload."""
+    import oracle
+
+    oracle.build()
+    threads = oracle.num_threads()
+    t0 = time.perf_counter()
+    oracle.run(w, 2, precision="f32")
+    per = (time.perf_counter() - t0) / 2
+    n = int(max(4, min(400, w.nt, seconds / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    oracle.run(w, n, precision="f32")
+    dt = time.perf_counter() - t0
+    return {"value": w.nx * w.nz * n / dt / 1e9, "unit": "Gpt/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} of {w.nt} time steps of the {w.nx}x{w.nz} {w.kind.upper()} "
+                      f"workload, FP32 CPU oracle, {threads} OpenMP threads"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+
+    w = workload(a)
+    oracle.build()
+    threads = oracle.num_threads()
+    t0 = time.perf_counter()
+    oracle.run(w, 2, precision="f32")
+    per = (time.perf_counter() - t0) / 2
+    # each bench step: a bounded sample of the solve (~8 s of CPU work)
+    n = int(max(2, min(200, w.nt, 8.0 / max(per, 1e-6))))
+    for _ in range(a.warmup):
+        oracle.run(w, n, precision="f32")
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        oracle.run(w, n, precision="f32")
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = w.nx * w.nz * n / (ms / 1e3) / 1e9
+    sample = (f"first {n} of {w.nt} time steps of the {w.nx}x{w.nz} {w.kind.upper()} workload per "
+              f"step; FP32 CPU restatement of the reference step (the Julia reference does not run "
+              f"here), {threads} OpenMP threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gpt/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(a), "nx": w.nx, "nz": w.nz, "nt_sampled": n},
+        "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from viscoelasticinversion_b200 import StepPlan
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = workload(a)
+    esize = 8 if a.precision == "f64" else 4
+    plan = StepPlan.for_workload(w, a.precision, device=local)
+    med = plan.medium_to_device(w.medium)
+    st = plan.zeros_state()
+    wav = torch.as_tensor(w.wavelets, dtype=plan.dtype, device=dev).contiguous()
+    traces = torch.zeros(2, len(w.receivers), w.nt, dtype=plan.dtype, device=dev)
+    stream = torch.cuda.current_stream()
+    kev = []
+
+    def one_step(record=False):
+        for t in st.values():
+            t.zero_()
+        plan.reset()
+        if record:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        plan.step(med, st, nsteps=w.nt, sources=w.sources, wavelets=wav, receivers=w.receivers,
+                  traces=traces, variant=a.variant)
+        if record:
+            e1.record(stream)
+            kev.append((e0, e1))
+
+    for _ in range(a.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    uuid = str(getattr(torch.cuda.get_device_properties(dev), "uuid", ""))
+    clocks = Clocks(uuid)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(a.steps):
+        one_step(record=True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(t0.elapsed_time(t1) / a.steps)
+    kern_ms = sum(e0.elapsed_time(e1) for e0, e1 in kev) / a.steps
+    pts = w.nx * w.nz * w.nt
+    value = world * pts / (ms / 1e3) / 1e9
+    launches_per_step = w.nt
+    mean_launch_s = kern_ms / 1e3 / launches_per_step
+    # algorithmic bytes of one fused launch: state read+written once, medium
+    # read once, CPML psi strips read+written once
+    bpt = w.bytes_per_point(esize)
+    wx = 2 * w.pml
+    hz = w.pml * (1 if w.free_surface else 2)
+    psi_bytes = 2 * esize * 4 * (wx * w.nz + w.nx * hz)
+    launch_bytes = bpt * w.nx * w.nz + psi_bytes
+    achieved = launch_bytes / mean_launch_s / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic(f"fused_{w.kind}_{w.nx}x{w.nz}")
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "Gpt/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": a.precision, "data": "synthetic",
+        "config": {"workload": workload_name(a), "nx": w.nx, "nz": w.nz, "nt": w.nt,
+                   "nsls": w.nsls, "medium": w.kind, "bytes_per_point": bpt,
+                   "l2": f"inputs larger than L2 ({launch_bytes / 1e6:.0f} MB per time step)",
+                   "parallelism": f"shot-parallel x{world}", "kernel_variant": a.variant},
+        "gpu_launches": a.steps * launches_per_step,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "bytes_per_launch": launch_bytes,
+                     "mean_launch_us": mean_launch_s * 1e6},
+        "clocks": clk,
+    }
+
+    if not a.no_e2e:
+        # end to end through vi_forward_host with pinned host buffers
+        npdt = np.float64 if a.precision == "f64" else np.float32
+        tdt = torch.float64 if a.precision == "f64" else torch.float32
+        med_h = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=npdt)).pin_memory()
+                 for k, v in w.medium.items()}
+        wav_h = torch.from_numpy(np.ascontiguousarray(w.wavelets, dtype=npdt)).pin_memory()
+        tr_h = torch.empty(2, len(w.receivers), w.nt, dtype=tdt).pin_memory()
+        h2d = sum(t.numel() * t.element_size() for t in med_h.values()) + wav_h.numel() * esize
+        d2h = tr_h.numel() * esize
+        for _ in range(max(1, a.warmup // 2)):
+            plan.forward_host(med_h, w.sources, wav_h, w.receivers, w.nt, traces_out=tr_h)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            plan.forward_host(med_h, w.sources, wav_h, w.receivers, w.nt, traces_out=tr_h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = max_over_ranks(e0.elapsed_time(e1) / a.steps)
+        out["e2e"] = {"value": world * pts / (ems / 1e3) / 1e9, "unit": "Gpt/s",
+                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ems,
+                      "api": "vi_forward_host"}
+        out["gpu_launches"] += a.steps * launches_per_step
+
+    if rank == 0 and world == 1 and not a.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(w, a.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/*
+ * visco_b200.h — C ABI of the B200 (sm_100a) 2D viscoelastic / anisotropic
+ * staggered-grid velocity–stress time step.
+ *
+ * The reference (haralddd/ViscoelasticInversion) is Julia; its hot path is the
+ * set of KernelAbstractions kernels in src/visco-kernels.jl,
+ * src/diff-funcs.jl, src/free-surface-kernels.jl and the custom_solver
+ * Solver/PointSource types.  Each entry point below names the reference item
+ * it replaces (file:line).  The reference binds nothing over an FFI; a Julia
+ * `ccall` veneer or the Python host package calls these.
+ *
+ * Conventions
+ *   - Arrays are x-fastest (Julia column-major [Nx,Nz]): element (i,j) of a
+ *     plane lives at i + j*nx, 0 <= i < nx, 0 <= j < nz.
+ *   - Staggering (Virieux): sxx, szz, rho, C, tau at (i, j); vx at (i+1/2, j);
+ *     vz at (i, j+1/2); sxz at (i+1/2, j+1/2).  Memory variables sit with the
+ *     stress component they drive.
+ *   - Only the update region U = [4, nx-4) x [4, nz-4) is ever written; cells
+ *     outside U stay as the caller left them (zero), as the reference's
+ *     `worksize = size - 2*pad` launch (visco-kernels.jl:95-98) does.
+ *   - With the free surface on, row 4 is the surface (sxx, szz, vx level) and
+ *     rows 0..3 hold the stress images.
+ *   - All calls return an int status (VI_OK = 0).  vi_last_error() gives the
+ *     message of the last failing call on the calling thread.  No C++
+ *     exception or device trap crosses this boundary.
+ *   - Pointers named *_dev are device pointers; *_host are host pointers.
+ *     The precision of every real array is the plan's precision (float for
+ *     VI_F32, double for VI_F64).
+ */
+#ifndef VISCO_B200_H
+#define VISCO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VI_ABI_VERSION 1
+#define VI_HALF 4          /* half-length of the 8th-order staggered stencil */
+#define VI_MAX_SLS 5       /* maximum number of standard linear solids */
+
+/* status codes */
+#define VI_OK 0
+#define VI_ERR_ARG 1        /* bad argument / configuration */
+#define VI_ERR_CFL 2        /* CFL condition violated */
+#define VI_ERR_BUDGET 3     /* HBM budget or capacity exceeded */
+#define VI_ERR_TIMEOUT 4    /* a bounded device wait gave up */
+#define VI_ERR_CUDA 5       /* CUDA runtime error */
+#define VI_ERR_NONFINITE 6  /* a non-finite value was detected */
+#define VI_ERR_STATE 7      /* call not valid in the object's current state */
+
+/* medium kinds (sciml_solver/Models.jl:3-43) */
+#define VI_MEDIUM_ISO 0     /* reads rho, c13 (= lambda), c55 (= mu), tau */
+#define VI_MEDIUM_VTI 1     /* reads rho, c11, c13, c33, c55, tau */
+#define VI_MEDIUM_TTI 2     /* reads rho, c11, c13, c15, c33, c35, c55, tau */
+
+#define VI_F32 0
+#define VI_F64 1
+
+/* source kinds */
+#define VI_SRC_EXPLOSIVE 0  /* sxx, szz += dt*amp*w(t) */
+#define VI_SRC_FORCE_X 1    /* vx += dt*b*amp*w(t)   (Source.jl:35-58 form) */
+#define VI_SRC_FORCE_Z 2    /* vz += dt*b*amp*w(t)   (ViscoelasticProblem.jl:165-171) */
+
+/* Plan configuration.  Mirrors Parameters(;Nx,Nz,dx,dz,dt,...)
+ * (sciml_solver/Parameters.jl:47-86), CPMLConfig (sciml_solver/CPML.jl:40-63)
+ * and QModel's tau_n (sciml_solver/Models.jl:90-102). */
+typedef struct vi_config {
+  int32_t nx, nz;
+  double dx, dz, dt;
+  int32_t medium;          /* VI_MEDIUM_* */
+  int32_t precision;       /* VI_F32 / VI_F64 */
+  int32_t nsls;            /* 0..VI_MAX_SLS */
+  int32_t free_surface;    /* 1: stress-imaging free surface at row VI_HALF */
+  double tau_sls[VI_MAX_SLS]; /* relaxation times tau_n of the mechanisms */
+  /* CPML */
+  int32_t pml_thickness;   /* cells, counted from the array edge */
+  int32_t pml_left, pml_right, pml_top, pml_bottom;
+  double pml_d0;           /* <= 0: Collino–Tsogka d0 from vmax and R */
+  double pml_vmax;
+  double pml_reflection;   /* R in d0 = -(p+1) vmax ln R / (2 L h) */
+  double pml_power;
+  double pml_alpha_max;
+  double pml_kappa_max;
+} vi_config;
+
+/* Medium planes (nx*nz each).  For VI_MEDIUM_ISO, c11 = c33 = c13 + 2*c55
+ * is derived on chip and c11/c15/c33/c35 are ignored. */
+typedef struct vi_medium {
+  const void *rho, *c11, *c13, *c15, *c33, *c35, *c55, *tau;
+} vi_medium;
+
+/* Wavefield state.  Maps both the reference's stacked Fields(s, M, v)
+ * arrays (visco-kernels.jl:102-106: s[Nx,Nz,3], v[Nx,Nz,2], M[Nx,Nz,N,3])
+ * and the custom Solver(vx,vz,sxx,szz,sxz) planes (custom_solver/Model.jl:4-10)
+ * without a copy.  m holds 3*nsls planes; plane (c*nsls + n) is memory
+ * variable n of component c (0 = xx, 1 = zz, 2 = xz), each m_plane_stride
+ * elements apart. */
+typedef struct vi_fields {
+  void *vx, *vz, *sxx, *szz, *sxz, *m;
+  int64_t m_plane_stride;
+} vi_fields;
+
+typedef struct vi_source {
+  int32_t i, j, kind;
+  int32_t pad_;
+  double amp;
+} vi_source;
+
+typedef struct vi_receiver {
+  int32_t i, j;            /* samples vx(i+1/2, j) and vz(i, j+1/2) */
+} vi_receiver;
+
+/* Shot description for the time loop.  wavelet_dev holds nsrc rows of
+ * wavelet_nt samples (plan precision); step it uses sample
+ * w[s*wavelet_nt + it] (zero when it >= wavelet_nt).  traces_dev receives
+ * 2*nrec rows of traces_nt samples: row r is vx of receiver r, row nrec+r is
+ * vz; step it writes column it (when it < traces_nt).  Index lists are host
+ * pointers copied by the call. */
+typedef struct vi_shot {
+  int32_t nsrc;
+  const vi_source *src_host;
+  const void *wavelet_dev;
+  int32_t wavelet_nt;
+  int32_t nrec;
+  const vi_receiver *rec_host;
+  void *traces_dev;
+  int32_t traces_nt;
+} vi_shot;
+
+typedef struct vi_plan vi_plan;
+
+/* ---- library ---------------------------------------------------------- */
+int vi_version(void);
+const char *vi_last_error(void);
+
+/* ---- plan ------------------------------------------------------------- */
+/* Builds the CPML profiles (CPML.jl:109-221, evaluated at the staggered
+ * positions), checks CFL and allocates the plan's device workspace (CPML
+ * psi strips).  Replaces the host set-up of Parameters(;...)
+ * (Parameters.jl:47-86) for the leapfrog path. */
+int vi_plan_create(const vi_config *cfg, vi_plan **out);
+int vi_plan_destroy(vi_plan *plan);
+/* Zeroes the plan's CPML memory variables (CPMLMemory, CPML.jl:246-263). */
+int vi_plan_reset(vi_plan *plan, void *stream);
+/* Bytes of device memory the plan holds. */
+int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
+
+/* ---- time stepping ------------------------------------------------------ */
+/* Advances the caller's wavefields by nsteps leapfrog steps starting at step
+ * index it0, in place, on `stream` (asynchronous).  One step = velocity
+ * update from the stress divergence (+ force sources, receivers sampled),
+ * then the SLS stress + memory-variable update (+ explosive sources), the
+ * free-surface condition and the stress images.  Replaces
+ * leapfrog_step!(fields, parameters, dt) (visco-kernels.jl:87-100) together
+ * with _vel_1Q! (:3-20), _stress_1Q! (:59-85), the free-surface kernels
+ * (free-surface-kernels.jl:16-213) and the CPML/ψ recursion
+ * (sciml_solver/CPML.jl:291-328).  `shot` may be NULL (no sources or
+ * receivers).  kernel_variant: 0 = tuned default, 1 = plain two-kernel
+ * path, 2 = fused single-kernel path. */
+int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
+            const vi_shot *shot, int32_t it0, int32_t nsteps,
+            int32_t kernel_variant, void *stream);
+
+/* One whole forward solve with host buffers: uploads the medium and the
+ * wavelets, runs nt steps from a zero state and downloads the traces and
+ * (optionally) the final wavefields.  Synchronous.  The end-to-end form of
+ * the time loop the reference leaves unwritten (call stack of
+ * leapfrog_step!, visco-kernels.jl:87-100). */
+int vi_forward_host(vi_plan *plan, const vi_medium *med_host,
+                    int32_t nsrc, const vi_source *src, const void *wavelet_host,
+                    int32_t nrec, const vi_receiver *rec, int32_t nt,
+                    void *traces_host, vi_fields *final_host);
+
+/* ---- staggered derivatives (diff-funcs.jl:3-32) ----------------------- */
+/* du = D(u) over the update region for one plane (device pointers, plan
+ * precision).  op: 0 = ddxp, 1 = ddxm, 2 = ddzp, 3 = ddzm.  h is the grid
+ * spacing along the operator's axis. */
+int vi_diff(int32_t precision, int32_t op, const void *u_dev, void *du_dev,
+            int32_t nx, int32_t nz, double h, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VISCO_B200_H */

@@ -1,0 +1,40 @@
+// plan.cuh — the plan object behind the C ABI (host side).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+struct vi_plan {
+  vi_config cfg;
+  int device = 0;
+  int Lx = 0, Rx = 0, Tz = 0, Bz = 0, wx = 0, hz = 0;
+  size_t esize = 4;  // bytes per real
+  // device workspace
+  void *psix = nullptr, *psiz = nullptr;  // kPsiPlanes planes each
+  long long psix_plane = 0, psiz_plane = 0;
+  int psi_cur = 0;  // which of the two psi sets holds the current state
+  void *tabx = nullptr, *tabz = nullptr;  // 6*nx and 6*nz reals
+  void *scratch = nullptr;                // plain path: 6 planes
+  void *alt = nullptr;                    // fused path: second v/sigma copy (5 planes)
+  // source / receiver lists (device, grown on demand)
+  void *dsrc = nullptr, *damp = nullptr, *drec = nullptr;
+  int src_cap = 0, rec_cap = 0;
+  // fused path: per-tile source / receiver lists (device, grown on demand)
+  void *tile_lists = nullptr;
+  size_t tile_lists_bytes = 0;
+  // forward_host buffers (device, grown on demand)
+  void *fwd = nullptr;
+  size_t fwd_bytes = 0;
+  size_t bytes = 0;  // device bytes held
+  // host copies of the CPML tables in double precision
+  std::vector<double> htx, htz;
+};
+
+namespace vb {
+int set_error(int code, const std::string &msg);
+int cuda_check(cudaError_t e, const char *what);
+// Grow-only device buffer.
+int ensure_buffer(vi_plan *p, void **buf, size_t *have, size_t need);
+}  // namespace vb
