@@ -249,7 +249,7 @@ def homogeneous_iso(nx=256, nz=256, dx=5.0, dt=0.5e-3, nt=1000, vp=3000.0, vs=17
         med["tau"] = np.full(shape, qf.tau_for(Q))
     t_unrelaxed = 1.0 + (med["tau"].max() if nsls else 0.0)
     vmax = vp * math.sqrt(t_unrelaxed)
-    js = VI_HALF if free_surface else 0
+    js = VI_HALF  # surface row, or the first row of the update region
     si, sj = src if src is not None else (nx // 2, nz // 2)
     return Workload(
         name=f"iso-homogeneous-{nx}x{nz}", nx=nx, nz=nz, dx=dx, dz=dx, dt=dt, nt=nt, kind="iso",
@@ -319,7 +319,7 @@ def layered(nx=2048, nz=1024, dx=5.0, dt=0.4e-3, nt=4000, kind="vti", seed=0, nl
     # fastest phase velocity: horizontal P in VTI, sqrt(max(C11, C33)/rho) bound for TTI
     cmax = np.maximum(med.get("c11", C11), med.get("c33", C33))
     vmax = float(np.sqrt(cmax / rho).max() * math.sqrt(1.0 + tmax))
-    js = VI_HALF if free_surface else 0
+    js = VI_HALF  # surface row, or the first row of the update region
     src_j = js + int(round(20.0 / dx))
     return Workload(
         name=f"{kind}-layered-{nx}x{nz}-seed{seed}", nx=nx, nz=nz, dx=dx, dz=dx, dt=dt, nt=nt,
