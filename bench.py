@@ -116,7 +116,7 @@ def measured_peaks():
 def ncu_traffic(name: str):
     """DRAM bytes per launch of the fused kernel from the committed ncu
     summary of this workload (profiles/), or None."""
-    f = ROOT / "profiles" / f"{name}.txt"
+    f = ROOT / "profiles" / f"{name}.ncu.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -264,7 +264,9 @@ def run_ours(a):
     launch_bytes = bpt * w.nx * w.nz + psi_bytes
     achieved = launch_bytes / mean_launch_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic(f"fused_{w.kind}_{w.nx}x{w.nz}")
+    kernel = plan.last_kernel()
+    kname = {"fused-tma": "k_fused_tma", "fused": "k_fused", "plain": "k_plain"}.get(kernel, kernel)
+    traffic = ncu_traffic(f"{kname}_{w.kind}_{w.nx}x{w.nz}")
 
     out = {
         "metric": METRIC, "value": value, "unit": "Gpt/s", "n_gpus": world, "steps": a.steps,
@@ -273,7 +275,8 @@ def run_ours(a):
         "config": {"workload": workload_name(a), "nx": w.nx, "nz": w.nz, "nt": w.nt,
                    "nsls": w.nsls, "medium": w.kind, "bytes_per_point": bpt,
                    "l2": f"inputs larger than L2 ({launch_bytes / 1e6:.0f} MB per time step)",
-                   "parallelism": f"shot-parallel x{world}", "kernel_variant": a.variant},
+                   "parallelism": f"shot-parallel x{world}", "kernel_variant": a.variant,
+                   "kernel": kname},
         "gpu_launches": a.steps * launches_per_step,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,

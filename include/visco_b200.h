@@ -146,6 +146,12 @@ int vi_plan_destroy(vi_plan *plan);
 int vi_plan_reset(vi_plan *plan, void *stream);
 /* Bytes of device memory the plan holds. */
 int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
+/* Synchronizes `stream` and reports (then clears) the plan's device error
+ * word: VI_ERR_TIMEOUT when a bounded in-kernel wait gave up.  Kernels never
+ * trap; this is how a device-side failure reaches the caller. */
+int vi_plan_status(vi_plan *plan, void *stream);
+/* Which kernel the last vi_step ran: 1 plain, 2 fused, 3 fused TMA-staged. */
+int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
 
 /* ---- time stepping ------------------------------------------------------ */
 /* Advances the caller's wavefields by nsteps leapfrog steps starting at step
@@ -157,8 +163,10 @@ int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
  * with _vel_1Q! (:3-20), _stress_1Q! (:59-85), the free-surface kernels
  * (free-surface-kernels.jl:16-213) and the CPML/ψ recursion
  * (sciml_solver/CPML.jl:291-328).  `shot` may be NULL (no sources or
- * receivers).  kernel_variant: 0 = tuned default, 1 = plain two-kernel
- * path, 2 = fused single-kernel path. */
+ * receivers).  kernel_variant: 0 = default (the TMA-staged fused kernel when
+ * rows, planes and pointers are 16-byte aligned, else the fused kernel),
+ * 1 = plain multi-kernel path (in place), 2 = fused kernel without TMA,
+ * 3 = TMA-staged fused kernel (VI_ERR_ARG when not eligible). */
 int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);

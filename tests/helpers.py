@@ -15,9 +15,10 @@ def rel_l2(a, b) -> float:
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
-def run_gpu(w, precision="f32", variant=2, chunks=None, nt=None):
+def run_gpu(w, precision="f32", variant=2, chunks=None, nt=None, info=None):
     """Runs w from rest on cuda:0 through vi_step; returns (traces, state)
-    as float64 numpy arrays."""
+    as float64 numpy arrays.  `info`, if a dict, receives the kernel the
+    plan ran."""
     nt = w.nt if nt is None else nt
     plan = StepPlan.for_workload(w, precision)
     med = plan.medium_to_device(w.medium)
@@ -30,7 +31,9 @@ def run_gpu(w, precision="f32", variant=2, chunks=None, nt=None):
         plan.step(med, st, nsteps=n, it0=it, sources=w.sources, wavelets=wav,
                   receivers=w.receivers, traces=traces, variant=variant)
         it += n
-    torch.cuda.synchronize()
+    plan.status()
+    if info is not None:
+        info["kernel"] = plan.last_kernel()
     out = {k: v.double().cpu().numpy() for k, v in st.items()}
     out["m"] = out["m"].reshape(-1, w.nz, w.nx)
     plan.close()

@@ -38,17 +38,48 @@ def oracle_run(oracle_lib, name):
     return _cache[name]
 
 
+KERNEL_OF_VARIANT = {1: "plain", 2: "fused", 3: "fused-tma"}
+
+
 @pytest.mark.parametrize("name", ["iso256", "vti256x128", "tti256x128", "iso-odd37x29"])
 @pytest.mark.parametrize("precision", ["f32", "f64"])
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_parity_with_oracle(oracle_lib, name, precision, variant):
     w, tr_ref, st_ref = oracle_run(oracle_lib, name)
     assert np.abs(tr_ref).max() > 0
-    tr, st = run_gpu(w, precision, variant)
+    if variant == 3 and (w.nx * (8 if precision == "f64" else 4)) % 16:
+        # rows not 16-byte aligned: the TMA kernel refuses, the default falls back
+        from viscoelasticinversion_b200 import ViError
+
+        with pytest.raises(ViError):
+            run_gpu(w, precision, 3)
+        info = {}
+        run_gpu(w, precision, 0, nt=4, info=info)
+        assert info["kernel"] == "fused"
+        return
+    info = {}
+    tr, st = run_gpu(w, precision, variant, info=info)
+    assert info["kernel"] == KERNEL_OF_VARIANT[variant]
     err = compare(tr, st, tr_ref, st_ref, w.nsls)
     print(name, precision, variant, err)
     bad = {k: v for k, v in err.items() if not v <= TOL[precision]}
     assert not bad, f"{name} {precision} variant {variant}: {err}"
+
+
+@pytest.mark.parametrize("kind", ["iso", "vti", "tti"])
+@pytest.mark.parametrize("nsls", [0, 1, 5])
+def test_tma_kernel_mechanism_counts(oracle_lib, kind, nsls):
+    """Every (medium, N_sls) instantiation of the TMA-staged kernel against
+    the oracle (FP32), including the shapes that fall back to 8-row tiles."""
+    w = media.layered(nx=192, nz=100, nt=200, kind=kind, seed=11, pml=12, nrec=16, nsls=nsls)
+    tr_ref, st_ref = oracle_lib.run(w, precision="f64")
+    info = {}
+    tr, st = run_gpu(w, "f32", 0, info=info)
+    err = compare(tr, st, tr_ref, st_ref, w.nsls)
+    assert max(err.values()) < 1e-5, (info, err)
+    trd, std = run_gpu(w, "f64", 0, info=info)
+    errd = compare(trd, std, tr_ref, st_ref, w.nsls)
+    assert max(errd.values()) < 1e-10, (info, errd)
 
 
 @pytest.mark.parametrize("kind", ["iso", "vti", "tti"])
@@ -57,7 +88,7 @@ def test_no_free_surface_with_top_cpml_and_force_sources(oracle_lib, kind):
     w.sources = [(80, 60, 1, 1.0), (81, 59, 2, -0.5), (40, 30, 0, 2.0), (80, 60, 2, 0.25)]
     w.wavelets = np.stack([w.wavelets[0]] * 4)
     tr_ref, st_ref = oracle_lib.run(w, precision="f64")
-    for variant in (1, 2):
+    for variant in (1, 2, 3):
         tr, st = run_gpu(w, "f64", variant)
         err = compare(tr, st, tr_ref, st_ref, w.nsls)
         assert max(err.values()) < 1e-10, (variant, err)
@@ -73,6 +104,10 @@ def test_chunked_stepping_equals_one_call():
     # the plain in-place path and the fused path interleave on one plan state
     tr3, st3 = run_gpu(w, "f32", 1, chunks=[150, 150])
     assert rel_l2(tr3, tr1) < 1e-5
+    # the two fused kernels (TMA-staged and not) produce the same result
+    tr4, st4 = run_gpu(w, "f32", 3)
+    tr5, st5 = run_gpu(w, "f32", 2)
+    assert rel_l2(tr4, tr5) < 1e-6
 
 
 def test_deterministic():

@@ -279,7 +279,7 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   rc = check_fields(p, f);
   if (rc) return rc;
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
-  if (variant < 0 || variant > 2) return set_error(VI_ERR_ARG, "unknown kernel variant");
+  if (variant < 0 || variant > 3) return set_error(VI_ERR_ARG, "unknown kernel variant");
   if (s && s->nrec > 0 && s->traces_nt > 0 && !s->traces_dev)
     return set_error(VI_ERR_ARG, "receivers need traces_dev");
   rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
@@ -318,9 +318,11 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
     for (int k = 0; k < nsteps; ++k) plain_step<T>(a, x, p->cfg.medium, it0 + k, st);
   } else {
-    rc = fused_steps<T>(p, a, s, it0, nsteps, st);
+    rc = fused_steps<T>(p, a, s, it0, nsteps, st, variant);
     if (rc) return rc;
+    p->last_kernel = p->last_used_tma ? 3 : 2;
   }
+  if (variant == 1) p->last_kernel = 1;
   return cuda_check(cudaGetLastError(), "step launch");
 }
 
@@ -371,6 +373,9 @@ extern "C" int vi_plan_create(const vi_config *cfg, vi_plan **out) {
     h = 0;
     if ((rc = ensure_buffer(p, &p->psiz, &h, kPsiPlanes * (size_t)p->psiz_plane * p->esize))) goto fail;
   }
+  h = 0;
+  if ((rc = ensure_buffer(p, &p->errflag, &h, 16))) goto fail;
+  if ((rc = cuda_check(cudaMemset(p->errflag, 0, 16), "zero error word"))) goto fail;
   rc = cfg->precision == VI_F64 ? upload_tables<double>(p) : upload_tables<float>(p);
   if (rc) goto fail;
   rc = vi_plan_reset(p, nullptr);
@@ -390,7 +395,7 @@ extern "C" int vi_plan_destroy(vi_plan *p) {
   cudaGetDevice(&prev);
   cudaSetDevice(p->device);
   void *bufs[] = {p->psix, p->psiz, p->tabx, p->tabz, p->scratch, p->alt,
-                  p->dsrc, p->damp, p->drec, p->tile_lists, p->fwd};
+                  p->dsrc, p->damp, p->drec, p->tile_lists, p->fwd, p->errflag};
   for (void *b : bufs)
     if (b) cudaFree(b);
   cudaSetDevice(prev);
@@ -406,6 +411,26 @@ extern "C" int vi_plan_reset(vi_plan *p, void *stream) {
     return rc;
   if (p->psiz && (rc = cuda_check(cudaMemsetAsync(p->psiz, 0, kPsiPlanes * (size_t)p->psiz_plane * p->esize, st), "reset psi z")))
     return rc;
+  return VI_OK;
+}
+
+extern "C" int vi_plan_status(vi_plan *p, void *stream) {
+  if (!p) return set_error(VI_ERR_ARG, "plan is NULL");
+  int rc = cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "plan status");
+  if (rc) return rc;
+  int flag = 0;
+  rc = cuda_check(cudaMemcpy(&flag, p->errflag, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
+  if (rc) return rc;
+  if (flag) {
+    cudaMemset(p->errflag, 0, sizeof(int));
+    return set_error(VI_ERR_TIMEOUT, "a bounded device wait gave up (tile staging did not complete)");
+  }
+  return VI_OK;
+}
+
+extern "C" int vi_plan_last_kernel(const vi_plan *p, int32_t *kernel) {
+  if (!p || !kernel) return set_error(VI_ERR_ARG, "NULL argument");
+  *kernel = p->last_kernel;
   return VI_OK;
 }
 
@@ -513,7 +538,9 @@ static int forward_host_impl(vi_plan *p, const vi_medium *mh, int nsrc, const vi
         if (rc) return rc;
       }
   }
-  return cuda_check(cudaDeviceSynchronize(), "forward");
+  rc = cuda_check(cudaDeviceSynchronize(), "forward");
+  if (rc) return rc;
+  return vi_plan_status(p, nullptr);
 }
 }  // namespace vb
 

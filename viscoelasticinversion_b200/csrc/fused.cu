@@ -9,9 +9,11 @@
 // recomputation never reads a value another CTA has already advanced.
 // Per step each cell's state and medium cross HBM once: reads of v, sigma,
 // M, psi and the medium, writes of v, sigma, M and psi.
+#include <cstdint>
 #include <vector>
 
 #include "fused.cuh"
+#include "fused_tma.cuh"
 #include "plan.cuh"
 
 namespace vb {
@@ -365,25 +367,17 @@ static int launch_fused_dispatch(int kind, const StepArgs<T> &a, const FusedExtr
   return set_error(VI_ERR_ARG, "unsupported medium / nsls combination");
 }
 
-template <int KIND>
-static void tile_counts(int nx, int nz, int &ntx, int &ntz) {
-  using G = FusedGeom<KIND>;
-  ntx = (nx - 2 * L + G::TX - 1) / G::TX;
-  ntz = (nz - 2 * L + G::TZ - 1) / G::TZ;
-}
-
-// Builds the per-tile CSR list of sources and receivers.  Force sources are
-// listed for every tile whose recomputed-velocity halo covers them;
-// explosive sources and receivers only for the owning tile.
-template <int KIND>
-static void build_tile_lists(int nx, int nz, const vi_shot *s, std::vector<int> &off,
-                             std::vector<int4> &ent) {
-  using G = FusedGeom<KIND>;
-  int ntx, ntz;
-  tile_counts<KIND>(nx, nz, ntx, ntz);
+// Builds the per-tile CSR list of sources and receivers for a TX x TZ
+// tiling whose recomputed-velocity halo is HV cells.  Force sources are
+// listed for every tile whose halo covers them; explosive sources and
+// receivers only for the owning tile.
+static void build_tile_lists(int nx, int nz, int TX, int TZ, int HV, const vi_shot *s,
+                             std::vector<int> &off, std::vector<int4> &ent, int &ntx, int &ntz) {
+  ntx = (nx - 2 * L + TX - 1) / TX;
+  ntz = (nz - 2 * L + TZ - 1) / TZ;
   const int ntiles = ntx * ntz;
   std::vector<std::vector<int4>> per(ntiles);
-  auto own_tile = [&](int i, int j) { return ((j - L) / G::TZ) * ntx + (i - L) / G::TX; };
+  auto own_tile = [&](int i, int j) { return ((j - L) / TZ) * ntx + (i - L) / TX; };
   if (s) {
     for (int q = 0; q < s->nsrc; ++q) {
       const vi_source &v = s->src_host[q];
@@ -392,13 +386,12 @@ static void build_tile_lists(int nx, int nz, const vi_shot *s, std::vector<int> 
         continue;
       }
       const int kind = v.kind == VI_SRC_FORCE_X ? TL_FORCE_X : TL_FORCE_Z;
-      const int bx0 = (v.i - L - G::HV) / G::TX - 1, bx1 = (v.i - L + G::HV) / G::TX;
-      const int bz0 = (v.j - L - G::HV) / G::TZ - 1, bz1 = (v.j - L + G::HV) / G::TZ;
+      const int bx0 = (v.i - L - HV) / TX - 1, bx1 = (v.i - L + HV) / TX;
+      const int bz0 = (v.j - L - HV) / TZ - 1, bz1 = (v.j - L + HV) / TZ;
       for (int bz = bz0 < 0 ? 0 : bz0; bz <= bz1 && bz < ntz; ++bz)
         for (int bx = bx0 < 0 ? 0 : bx0; bx <= bx1 && bx < ntx; ++bx) {
-          const int x0 = L + bx * G::TX, z0 = L + bz * G::TZ;
-          if (v.i >= x0 - G::HV && v.i < x0 + G::TX + G::HV && v.j >= z0 - G::HV &&
-              v.j < z0 + G::TZ + G::HV)
+          const int x0 = L + bx * TX, z0 = L + bz * TZ;
+          if (v.i >= x0 - HV && v.i < x0 + TX + HV && v.j >= z0 - HV && v.j < z0 + TZ + HV)
             per[bz * ntx + bx].push_back(make_int4(v.i, v.j, q, kind));
         }
     }
@@ -416,9 +409,53 @@ static void build_tile_lists(int nx, int nz, const vi_shot *s, std::vector<int> 
   off[ntiles] = (int)ent.size();
 }
 
+static bool aligned16(const void *ptr) { return ((uintptr_t)ptr & 15) == 0; }
+
+// Tensor maps of one ping-pong parity: the input state (sigma, v, M) and the
+// medium.
+template <typename T>
+static int encode_parity(TmaMaps &m, const TmaBoxes &b, const vi_config &c, T *const in[5],
+                         const T *min, long long mstride, const StepArgs<T> &a) {
+  const int e = sizeof(T), nx = c.nx, nz = c.nz;
+  int rc;
+  if ((rc = encode_map(&m.sxx, in[2], e, nx, nz, 1, 0, b.SWp, b.SH, 1))) return rc;
+  if ((rc = encode_map(&m.szz, in[3], e, nx, nz, 1, 0, b.SWp, b.SH, 1))) return rc;
+  if ((rc = encode_map(&m.sxz, in[4], e, nx, nz, 1, 0, b.SWp, b.SH, 1))) return rc;
+  if ((rc = encode_map(&m.vx, in[0], e, nx, nz, 1, 0, b.VWp, b.VH, 1))) return rc;
+  if ((rc = encode_map(&m.vz, in[1], e, nx, nz, 1, 0, b.VWp, b.VH, 1))) return rc;
+  if ((rc = encode_map(&m.rho, a.rho, e, nx, nz, 1, 0, b.RWp, b.RH, 1))) return rc;
+  if (c.nsls > 0) {
+    if ((rc = encode_map(&m.m, min, e, nx, nz, b.NM, mstride, b.MW, b.MH, b.NM))) return rc;
+    const bool tti = c.medium == VI_MEDIUM_TTI;
+    if ((rc = encode_map(&m.tau, a.tau, e, nx, nz, 1, 0, tti ? b.MW : b.CW, tti ? b.MH : b.CH, 1)))
+      return rc;
+  }
+  const T *slots[6];
+  int n = 0;
+  if (c.medium == VI_MEDIUM_ISO) {
+    slots[n++] = a.c13;
+    slots[n++] = a.c55;
+  } else if (c.medium == VI_MEDIUM_VTI) {
+    slots[n++] = a.c11;
+    slots[n++] = a.c13;
+    slots[n++] = a.c33;
+    slots[n++] = a.c55;
+  } else {
+    slots[n++] = a.c11;
+    slots[n++] = a.c13;
+    slots[n++] = a.c15;
+    slots[n++] = a.c33;
+    slots[n++] = a.c35;
+    slots[n++] = a.c55;
+  }
+  for (int k = 0; k < n; ++k)
+    if ((rc = encode_map(&m.c[k], slots[k], e, nx, nz, 1, 0, b.CW, b.CH, 1))) return rc;
+  return VI_OK;
+}
+
 template <typename T>
 int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps,
-                cudaStream_t st) {
+                cudaStream_t st, int mode) {
   const vi_config &c = p->cfg;
   const int kind = c.medium;
   const size_t np = (size_t)c.nx * c.nz;
@@ -434,22 +471,49 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     rc = cuda_check(cudaMemsetAsync(p->alt, 0, nstate * np * sizeof(T), st), "zero alt state");
     if (rc) return rc;
   }
+  T *user[5] = {a.vx, a.vz, a.sxx, a.szz, a.sxz};
+  T *user_m = a.m;
+  const long long user_ms = a.mstride;
+  T *alt = (T *)p->alt;
+  T *alt_st[5];
+  for (int q = 0; q < 5; ++q) alt_st[q] = alt + q * np;
+
+  // TMA eligibility: 16-byte aligned rows, planes and bases
+  const TmaBoxes bx = tma_boxes(kind, c.nsls, (int)sizeof(T));
+  bool use_tma = mode != 2 && bx.ok && ((size_t)c.nx * sizeof(T)) % 16 == 0 &&
+                 (np * sizeof(T)) % 16 == 0;
+  const void *ptrs[] = {user[0], user[1], user[2], user[3], user[4], a.rho, a.c11, a.c13,
+                        a.c15,   a.c33,   a.c35,   a.c55,   a.tau,   user_m};
+  for (const void *q : ptrs)
+    if (q && !aligned16(q)) use_tma = false;
+  if (c.nsls > 0 && ((size_t)user_ms * sizeof(T)) % 16 != 0) use_tma = false;
+  if (mode == 3 && !use_tma)
+    return set_error(VI_ERR_ARG, "TMA-staged step needs 16-byte aligned rows and planes");
+
+  int TX, TZ, HV;
+  if (use_tma) {
+    TX = bx.TX;
+    TZ = bx.TZ;
+    HV = bx.HV;
+  } else if (kind == VI_MEDIUM_TTI) {
+    TX = FusedGeom<VI_MEDIUM_TTI>::TX;
+    TZ = FusedGeom<VI_MEDIUM_TTI>::TZ;
+    HV = FusedGeom<VI_MEDIUM_TTI>::HV;
+  } else {
+    TX = FusedGeom<VI_MEDIUM_ISO>::TX;
+    TZ = FusedGeom<VI_MEDIUM_ISO>::TZ;
+    HV = FusedGeom<VI_MEDIUM_ISO>::HV;
+  }
   int ntx, ntz;
   std::vector<int> off;
   std::vector<int4> ent;
-  if (kind == VI_MEDIUM_TTI) {
-    tile_counts<VI_MEDIUM_TTI>(c.nx, c.nz, ntx, ntz);
-    build_tile_lists<VI_MEDIUM_TTI>(c.nx, c.nz, s, off, ent);
-  } else {
-    tile_counts<VI_MEDIUM_ISO>(c.nx, c.nz, ntx, ntz);
-    build_tile_lists<VI_MEDIUM_ISO>(c.nx, c.nz, s, off, ent);
-  }
+  build_tile_lists(c.nx, c.nz, TX, TZ, HV, s, off, ent, ntx, ntz);
   const int ntiles = ntx * ntz;
-  const size_t lbytes = off.size() * sizeof(int) + 16 + ent.size() * sizeof(int4);
+  const size_t ent_off = (off.size() * sizeof(int) + 15) / 16 * 16;
+  const size_t lbytes = ent_off + ent.size() * sizeof(int4) + 16;
   int rc = ensure_buffer(p, &p->tile_lists, &p->tile_lists_bytes, lbytes);
   if (rc) return rc;
   int *d_off = (int *)p->tile_lists;
-  const size_t ent_off = (off.size() * sizeof(int) + 15) / 16 * 16;
   int4 *d_ent = (int4 *)((char *)p->tile_lists + ent_off);
   rc = cuda_check(cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st),
                   "copy tile offsets");
@@ -462,6 +526,12 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   rc = cuda_check(cudaStreamSynchronize(st), "stage tile lists");
   if (rc) return rc;
 
+  TmaMaps maps[2];
+  if (use_tma) {
+    if ((rc = encode_parity<T>(maps[0], bx, c, user, user_m, user_ms, a))) return rc;
+    if ((rc = encode_parity<T>(maps[1], bx, c, alt_st, alt + 5 * np, (long long)np, a))) return rc;
+  }
+
   FusedExtras<T> x;
   x.ntx = ntx;
   x.fs = c.free_surface;
@@ -473,19 +543,13 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   x.traces = (s && s->nrec) ? (T *)s->traces_dev : nullptr;
   x.tnt = (s && s->nrec) ? s->traces_nt : 0;
   x.nrec = s ? s->nrec : 0;
+  x.err = (int *)p->errflag;
 
-  T *user[5] = {a.vx, a.vz, a.sxx, a.szz, a.sxz};
-  T *user_m = a.m;
-  const long long user_ms = a.mstride;
-  T *alt = (T *)p->alt;
   T *psix0 = (T *)p->psix, *psiz0 = (T *)p->psiz;
   for (int k = 0; k < nsteps; ++k) {
     const bool from_user = (k % 2) == 0;
-    T *in[5], *out[5];
-    for (int q = 0; q < 5; ++q) {
-      in[q] = from_user ? user[q] : alt + q * np;
-      out[q] = from_user ? alt + q * np : user[q];
-    }
+    T *const *in = from_user ? user : alt_st;
+    T *const *out = from_user ? alt_st : user;
     a.vx = in[0]; a.vz = in[1]; a.sxx = in[2]; a.szz = in[3]; a.sxz = in[4];
     a.vx_o = out[0]; a.vz_o = out[1]; a.sxx_o = out[2]; a.szz_o = out[3]; a.sxz_o = out[4];
     a.m = from_user ? user_m : alt + 5 * np;
@@ -498,14 +562,15 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     a.psiz = psiz0 ? psiz0 + cur * kPsiPerSet * p->psiz_plane : nullptr;
     a.psiz_o = psiz0 ? psiz0 + (1 - cur) * kPsiPerSet * p->psiz_plane : nullptr;
     x.it = it0 + k;
-    rc = launch_fused_dispatch<T>(kind, a, x, ntiles, st);
+    rc = use_tma ? launch_fused_tma<T>(kind, a, x, maps[from_user ? 0 : 1], ntiles, st)
+                 : launch_fused_dispatch<T>(kind, a, x, ntiles, st);
     if (rc) return rc;
     p->psi_cur = 1 - cur;
   }
   if (nsteps % 2 == 1) {
     // result sits in the plan's copy: bring it back to the caller's fields
     for (int q = 0; q < 5; ++q) {
-      rc = cuda_check(cudaMemcpyAsync(user[q], alt + q * np, np * sizeof(T), cudaMemcpyDeviceToDevice, st),
+      rc = cuda_check(cudaMemcpyAsync(user[q], alt_st[q], np * sizeof(T), cudaMemcpyDeviceToDevice, st),
                       "copy back fields");
       if (rc) return rc;
     }
@@ -516,10 +581,11 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
       if (rc) return rc;
     }
   }
+  p->last_used_tma = use_tma;
   return VI_OK;
 }
 
-template int fused_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t);
-template int fused_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int, cudaStream_t);
+template int fused_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t, int);
+template int fused_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int, cudaStream_t, int);
 
 }  // namespace vb

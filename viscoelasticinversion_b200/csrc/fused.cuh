@@ -35,13 +35,16 @@ struct FusedExtras {
   int wnt;
   T *traces;
   int tnt, nrec;
+  int *err;                // device error word (bounded waits that gave up)
 };
 
 // Runs nsteps fused steps, ping-ponging between the caller's fields (in
 // `a`) and the plan's second state copy; leaves the result in the caller's
-// fields.
+// fields.  mode 0: TMA-staged kernel when the grid and every pointer are
+// 16-byte aligned, else the non-TMA kernel; 2: non-TMA; 3: TMA (error when
+// not eligible).
 template <typename T>
 int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps,
-                cudaStream_t st);
+                cudaStream_t st, int mode);
 
 }  // namespace vb

@@ -1,0 +1,94 @@
+// fused_tma.cuh — shared-memory layout and host interface of the TMA-staged
+// fused step.
+#pragma once
+
+#include <cuda.h>
+
+#include "common.cuh"
+#include "fused.cuh"
+
+namespace vb {
+
+constexpr int kSmemLimit = 227 * 1024;  // per-CTA dynamic shared memory on sm_100
+
+template <typename T>
+constexpr int r128(int n) {  // round an element count up to 128 bytes
+  return (int)((((long long)n * (long long)sizeof(T) + 127) / 128) * 128 / (long long)sizeof(T));
+}
+
+// Every operand of one TX x TZ tile, staged by TMA boxes (x extent padded to
+// 4 elements so each box starts on a 16-byte boundary).
+template <typename T, int KIND, int NSLS, int TZ_>
+struct TmaLayout {
+  static constexpr int TX = 64, TZ = TZ_, NT = 256;
+  static constexpr bool TTI = KIND == VI_MEDIUM_TTI;
+  static constexpr int HV = TTI ? 5 : 4;        // halo of recomputed velocities
+  static constexpr int HS = HV + 4;              // halo of staged stresses
+  static constexpr int HVP = (HV + 3) / 4 * 4;   // x padding to 16-byte boxes
+  static constexpr int HSP = (HS + 3) / 4 * 4;
+  static constexpr int NM = 3 * NSLS;
+  static constexpr int NC = KIND == VI_MEDIUM_ISO ? 2 : (KIND == VI_MEDIUM_VTI ? 4 : 6);
+  // boxes (x extent, z extent)
+  static constexpr int SWp = TX + 2 * HSP, SH = TZ + 2 * HS;        // sigma
+  static constexpr int VWp = TX + 2 * HVP, VH = TZ + 2 * HV;        // velocity
+  static constexpr int VW = TX + 2 * HV;                            // computed velocity width
+  static constexpr int RWp = TX + 2 * HVP + 4, RH = TZ + 2 * HV + 1;  // rho
+  static constexpr int MX0 = TTI ? -4 : 0, MZ0 = TTI ? -1 : 0;      // M / tau box origin
+  static constexpr int MW = TTI ? TX + 8 : TX, MH = TTI ? TZ + 2 : TZ;
+  static constexpr int CW = TX + 4, CH = TZ + 1;                    // coefficients (+1 ring)
+  static constexpr int EW = TX + 2, EH = TZ + 2;                    // TTI effective rates
+  // plane sizes (elements, 128-byte aligned)
+  static constexpr int PS = r128<T>(SWp * SH), PV = r128<T>(VWp * VH), PR = r128<T>(RWp * RH);
+  static constexpr int PM = r128<T>(MW * MH * (NM > 0 ? NM : 1));
+  static constexpr int PC = r128<T>(CW * CH);
+  static constexpr int PT = TTI ? r128<T>(MW * MH) : PC;
+  static constexpr int PE = r128<T>(EW * EH);
+  // offsets (elements) after the 128-byte barrier slot
+  static constexpr int O_SXX = 128 / (int)sizeof(T), O_SZZ = O_SXX + PS, O_SXZ = O_SZZ + PS;
+  static constexpr int O_VX = O_SXZ + PS, O_VZ = O_VX + PV, O_RHO = O_VZ + PV;
+  static constexpr int O_M = O_RHO + PR;
+  static constexpr int O_C = O_M + (NSLS > 0 ? PM : 0);
+  static constexpr int O_TAU = O_C + NC * PC;
+  static constexpr int O_E = O_TAU + (NSLS > 0 ? PT : 0);
+  static constexpr int ELEMS = O_E + (TTI ? 3 * PE : 0);
+  static constexpr int BYTES = ELEMS * (int)sizeof(T);
+  // transaction bytes of all boxes of one tile
+  static constexpr int TX_BYTES =
+      (int)sizeof(T) * (3 * SWp * SH + 2 * VWp * VH + RWp * RH + (NSLS > 0 ? MW * MH * NM : 0) +
+                        NC * CW * CH + (NSLS > 0 ? (TTI ? MW * MH : CW * CH) : 0));
+  static constexpr bool FITS = BYTES <= kSmemLimit;
+};
+
+// Tile height: 16 rows when the staged operands fit, else 8.
+template <typename T, int KIND, int NSLS>
+struct TmaPick {
+  static constexpr int TZ = TmaLayout<T, KIND, NSLS, 16>::FITS ? 16 : 8;
+  using Lay = TmaLayout<T, KIND, NSLS, TZ>;
+  static constexpr bool OK = Lay::FITS;
+};
+
+// Tensor maps of one ping-pong parity.  Coefficient slot order per kind:
+// ISO (c13, c55), VTI (c11, c13, c33, c55), TTI (c11, c13, c15, c33, c35, c55).
+struct TmaMaps {
+  CUtensorMap sxx, szz, sxz, vx, vz, rho, m, tau;
+  CUtensorMap c[6];
+};
+
+// Tile and box geometry the host needs (tile lists, grid size, tensor-map
+// boxes) for a medium kind, mechanism count and element size.
+struct TmaBoxes {
+  int TX, TZ, HV, HS, HVP, HSP;
+  int SWp, SH, VWp, VH, RWp, RH, MX0, MZ0, MW, MH, NM, CW, CH, NC;
+  bool ok;
+};
+TmaBoxes tma_boxes(int kind, int nsls, int esize);
+
+template <typename T>
+int launch_fused_tma(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
+                     const TmaMaps &maps, int ntiles, cudaStream_t st);
+
+// Encodes a 2D (depth = 1) or 3D tensor map over an x-fastest array.
+int encode_map(CUtensorMap *map, const void *base, int esize, int nx, int nz, long long depth,
+               long long plane_stride_elems, int box_x, int box_z, int box_d);
+
+}  // namespace vb

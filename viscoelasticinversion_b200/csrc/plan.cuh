@@ -15,6 +15,9 @@ struct vi_plan {
   void *psix = nullptr, *psiz = nullptr;  // kPsiPlanes planes each
   long long psix_plane = 0, psiz_plane = 0;
   int psi_cur = 0;  // which of the two psi sets holds the current state
+  void *errflag = nullptr;     // device error word written by bounded waits
+  bool last_used_tma = false;  // the last fused call ran the TMA-staged kernel
+  int last_kernel = 0;         // 1 plain, 2 fused, 3 fused TMA-staged
   void *tabx = nullptr, *tabz = nullptr;  // 6*nx and 6*nz reals
   void *scratch = nullptr;                // plain path: 6 planes
   void *alt = nullptr;                    // fused path: second v/sigma copy (5 planes)

@@ -132,6 +132,15 @@ class StepPlan:
     def reset(self, stream=None):
         check(lib().vi_plan_reset(self._h, _stream_handle(stream)))
 
+    def status(self, stream=None):
+        """Synchronizes and raises if a bounded in-kernel wait gave up."""
+        check(lib().vi_plan_status(self._h, _stream_handle(stream)))
+
+    def last_kernel(self) -> str:
+        k = C.c_int32()
+        check(lib().vi_plan_last_kernel(self._h, C.byref(k)))
+        return {0: "none", 1: "plain", 2: "fused", 3: "fused-tma"}[k.value]
+
     def zeros_state(self) -> dict:
         """Zeroed device state {vx, vz, sxx, szz, sxz, m}."""
         kw = dict(device=self.device, dtype=self.dtype)
