@@ -7,6 +7,7 @@
 #include "fused.cuh"
 #include "plain.cuh"
 #include "plan.cuh"
+#include "split.cuh"
 
 namespace vb {
 
@@ -279,7 +280,7 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   rc = check_fields(p, f);
   if (rc) return rc;
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
-  if (variant < 0 || variant > 3) return set_error(VI_ERR_ARG, "unknown kernel variant");
+  if (variant < 0 || variant > 5) return set_error(VI_ERR_ARG, "unknown kernel variant");
   if (s && s->nrec > 0 && s->traces_nt > 0 && !s->traces_dev)
     return set_error(VI_ERR_ARG, "receivers need traces_dev");
   rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
@@ -317,10 +318,14 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     if (a.psix) a.psix = a.psix_o = (T *)p->psix + cur * kPsiPerSet * p->psix_plane;
     if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
     for (int k = 0; k < nsteps; ++k) plain_step<T>(a, x, p->cfg.medium, it0 + k, st);
+  } else if (variant == 5 || (variant == 0 && split_eligible<T>(p, a))) {
+    rc = split_steps<T>(p, a, s, it0, nsteps, st);
+    if (rc) return rc;
+    p->last_kernel = 5;
   } else {
     rc = fused_steps<T>(p, a, s, it0, nsteps, st, variant);
     if (rc) return rc;
-    p->last_kernel = p->last_used_tma ? 3 : 2;
+    p->last_kernel = p->last_used_tma ? (variant == 4 ? 4 : 3) : 2;
   }
   if (variant == 1) p->last_kernel = 1;
   return cuda_check(cudaGetLastError(), "step launch");
@@ -342,6 +347,11 @@ extern "C" int vi_plan_create(const vi_config *cfg, vi_plan **out) {
   vi_plan *p = new vi_plan();
   p->cfg = *cfg;
   cudaGetDevice(&p->device);
+  if (cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess ||
+      p->nsm <= 0) {
+    cudaGetLastError();
+    p->nsm = 148;
+  }
   p->esize = cfg->precision == VI_F64 ? 8 : 4;
   const int Lp = cfg->pml_thickness;
   p->Lx = (Lp > 0 && cfg->pml_left) ? Lp : 0;

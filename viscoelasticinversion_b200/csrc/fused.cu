@@ -371,8 +371,8 @@ static int launch_fused_dispatch(int kind, const StepArgs<T> &a, const FusedExtr
 // tiling whose recomputed-velocity halo is HV cells.  Force sources are
 // listed for every tile whose halo covers them; explosive sources and
 // receivers only for the owning tile.
-static void build_tile_lists(int nx, int nz, int TX, int TZ, int HV, const vi_shot *s,
-                             std::vector<int> &off, std::vector<int4> &ent, int &ntx, int &ntz) {
+void build_tile_lists(int nx, int nz, int TX, int TZ, int HV, const vi_shot *s,
+                      std::vector<int> &off, std::vector<int4> &ent, int &ntx, int &ntz) {
   ntx = (nx - 2 * L + TX - 1) / TX;
   ntz = (nz - 2 * L + TZ - 1) / TZ;
   const int ntiles = ntx * ntz;
@@ -407,6 +407,26 @@ static void build_tile_lists(int nx, int nz, int TX, int TZ, int HV, const vi_sh
     ent.insert(ent.end(), per[t].begin(), per[t].end());
   }
   off[ntiles] = (int)ent.size();
+}
+
+int stage_tile_lists(vi_plan *p, const std::vector<int> &off, const std::vector<int4> &ent,
+                     cudaStream_t st, int **d_off, int4 **d_ent) {
+  const size_t ent_off = (off.size() * sizeof(int) + 15) / 16 * 16;
+  const size_t lbytes = ent_off + ent.size() * sizeof(int4) + 16;
+  int rc = ensure_buffer(p, &p->tile_lists, &p->tile_lists_bytes, lbytes);
+  if (rc) return rc;
+  *d_off = (int *)p->tile_lists;
+  *d_ent = (int4 *)((char *)p->tile_lists + ent_off);
+  rc = cuda_check(cudaMemcpyAsync(*d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+                  "copy tile offsets");
+  if (rc) return rc;
+  if (!ent.empty()) {
+    rc = cuda_check(cudaMemcpyAsync(*d_ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice, st),
+                    "copy tile entries");
+    if (rc) return rc;
+  }
+  // the host vectors die at return: wait for the pageable copies
+  return cuda_check(cudaStreamSynchronize(st), "stage tile lists");
 }
 
 static bool aligned16(const void *ptr) { return ((uintptr_t)ptr & 15) == 0; }
@@ -479,15 +499,17 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   for (int q = 0; q < 5; ++q) alt_st[q] = alt + q * np;
 
   // TMA eligibility: 16-byte aligned rows, planes and bases
-  const TmaBoxes bx = tma_boxes(kind, c.nsls, (int)sizeof(T));
-  bool use_tma = mode != 2 && bx.ok && ((size_t)c.nx * sizeof(T)) % 16 == 0 &&
+  const bool persist = mode != 4;
+  const TmaBoxes bx = tma_boxes(kind, c.nsls, (int)sizeof(T), persist);
+  // (4-cell groups never straddle the update-region edge when nx % 4 == 0)
+  bool use_tma = mode != 2 && bx.ok && c.nx % 4 == 0 && ((size_t)c.nx * sizeof(T)) % 16 == 0 &&
                  (np * sizeof(T)) % 16 == 0;
   const void *ptrs[] = {user[0], user[1], user[2], user[3], user[4], a.rho, a.c11, a.c13,
                         a.c15,   a.c33,   a.c35,   a.c55,   a.tau,   user_m};
   for (const void *q : ptrs)
     if (q && !aligned16(q)) use_tma = false;
   if (c.nsls > 0 && ((size_t)user_ms * sizeof(T)) % 16 != 0) use_tma = false;
-  if (mode == 3 && !use_tma)
+  if ((mode == 3 || mode == 4) && !use_tma)
     return set_error(VI_ERR_ARG, "TMA-staged step needs 16-byte aligned rows and planes");
 
   int TX, TZ, HV;
@@ -509,21 +531,9 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   std::vector<int4> ent;
   build_tile_lists(c.nx, c.nz, TX, TZ, HV, s, off, ent, ntx, ntz);
   const int ntiles = ntx * ntz;
-  const size_t ent_off = (off.size() * sizeof(int) + 15) / 16 * 16;
-  const size_t lbytes = ent_off + ent.size() * sizeof(int4) + 16;
-  int rc = ensure_buffer(p, &p->tile_lists, &p->tile_lists_bytes, lbytes);
-  if (rc) return rc;
-  int *d_off = (int *)p->tile_lists;
-  int4 *d_ent = (int4 *)((char *)p->tile_lists + ent_off);
-  rc = cuda_check(cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st),
-                  "copy tile offsets");
-  if (rc) return rc;
-  if (!ent.empty()) {
-    rc = cuda_check(cudaMemcpyAsync(d_ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice, st),
-                    "copy tile entries");
-    if (rc) return rc;
-  }
-  rc = cuda_check(cudaStreamSynchronize(st), "stage tile lists");
+  int *d_off = nullptr;
+  int4 *d_ent = nullptr;
+  int rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent);
   if (rc) return rc;
 
   TmaMaps maps[2];
@@ -562,7 +572,7 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     a.psiz = psiz0 ? psiz0 + cur * kPsiPerSet * p->psiz_plane : nullptr;
     a.psiz_o = psiz0 ? psiz0 + (1 - cur) * kPsiPerSet * p->psiz_plane : nullptr;
     x.it = it0 + k;
-    rc = use_tma ? launch_fused_tma<T>(kind, a, x, maps[from_user ? 0 : 1], ntiles, st)
+    rc = use_tma ? launch_fused_tma<T>(kind, a, x, maps[from_user ? 0 : 1], ntiles, p->nsm, persist, st)
                  : launch_fused_dispatch<T>(kind, a, x, ntiles, st);
     if (rc) return rc;
     p->psi_cur = 1 - cur;

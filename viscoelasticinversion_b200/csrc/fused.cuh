@@ -1,5 +1,7 @@
 // fused.cuh — host interface of the fused single-kernel step.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 struct vi_plan;
@@ -46,5 +48,13 @@ struct FusedExtras {
 template <typename T>
 int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps,
                 cudaStream_t st, int mode);
+
+// Per-tile CSR list of sources and receivers for a TX x TZ tiling whose
+// recomputed-velocity halo is HV cells (0 for the split kernels).
+void build_tile_lists(int nx, int nz, int TX, int TZ, int HV, const vi_shot *s,
+                      std::vector<int> &off, std::vector<int4> &ent, int &ntx, int &ntz);
+// Copies the lists into the plan's device buffer (synchronizes `st`).
+int stage_tile_lists(vi_plan *p, const std::vector<int> &off, const std::vector<int4> &ent,
+                     cudaStream_t st, int **d_off, int4 **d_ent);
 
 }  // namespace vb

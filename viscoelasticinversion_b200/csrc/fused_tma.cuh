@@ -17,10 +17,16 @@ constexpr int r128(int n) {  // round an element count up to 128 bytes
 }
 
 // Every operand of one TX x TZ tile, staged by TMA boxes (x extent padded to
-// 4 elements so each box starts on a 16-byte boundary).
-template <typename T, int KIND, int NSLS, int TZ_>
+// 4 elements so each box starts on a 16-byte boundary), in STAGES buffers.
+// With two stages the kernel is persistent (one CTA per SM) and loads the
+// next tile while computing the current one.
+template <typename T, int KIND, int NSLS, int TZ_, int STAGES_>
 struct TmaLayout {
-  static constexpr int TX = 64, TZ = TZ_, NT = 256;
+  static constexpr int TX = 64, TZ = TZ_, STAGES = STAGES_;
+  static constexpr int NT = STAGES == 2 ? 512 : 256;
+  // cells per thread group in the stress stage: the persistent form has
+  // twice the threads, so it splits the tile into 2-wide groups
+  static constexpr int SWID = STAGES == 2 ? 2 : 4;
   static constexpr bool TTI = KIND == VI_MEDIUM_TTI;
   static constexpr int HV = TTI ? 5 : 4;        // halo of recomputed velocities
   static constexpr int HS = HV + 4;              // halo of staged stresses
@@ -36,20 +42,23 @@ struct TmaLayout {
   static constexpr int MX0 = TTI ? -4 : 0, MZ0 = TTI ? -1 : 0;      // M / tau box origin
   static constexpr int MW = TTI ? TX + 8 : TX, MH = TTI ? TZ + 2 : TZ;
   static constexpr int CW = TX + 4, CH = TZ + 1;                    // coefficients (+1 ring)
-  static constexpr int EW = TX + 2, EH = TZ + 2;                    // TTI effective rates
+  static constexpr int EW = TX + 8, EH = TZ + 2;  // TTI effective rates, origin (x0-4, z0-1)
   // plane sizes (elements, 128-byte aligned)
   static constexpr int PS = r128<T>(SWp * SH), PV = r128<T>(VWp * VH), PR = r128<T>(RWp * RH);
   static constexpr int PM = r128<T>(MW * MH * (NM > 0 ? NM : 1));
   static constexpr int PC = r128<T>(CW * CH);
   static constexpr int PT = TTI ? r128<T>(MW * MH) : PC;
   static constexpr int PE = r128<T>(EW * EH);
-  // offsets (elements) after the 128-byte barrier slot
-  static constexpr int O_SXX = 128 / (int)sizeof(T), O_SZZ = O_SXX + PS, O_SXZ = O_SZZ + PS;
-  static constexpr int O_VX = O_SXZ + PS, O_VZ = O_VX + PV, O_RHO = O_VZ + PV;
-  static constexpr int O_M = O_RHO + PR;
-  static constexpr int O_C = O_M + (NSLS > 0 ? PM : 0);
-  static constexpr int O_TAU = O_C + NC * PC;
-  static constexpr int O_E = O_TAU + (NSLS > 0 ? PT : 0);
+  // offsets inside one stage
+  static constexpr int S_SXX = 0, S_SZZ = PS, S_SXZ = 2 * PS;
+  static constexpr int S_VX = 3 * PS, S_VZ = S_VX + PV, S_RHO = S_VZ + PV;
+  static constexpr int S_M = S_RHO + PR;
+  static constexpr int S_C = S_M + (NSLS > 0 ? PM : 0);
+  static constexpr int S_TAU = S_C + NC * PC;
+  static constexpr int STAGE = S_TAU + (NSLS > 0 ? PT : 0);
+  // whole buffer: 128-byte barrier slot, the stages, the TTI rate planes
+  static constexpr int O_STAGE = 128 / (int)sizeof(T);
+  static constexpr int O_E = O_STAGE + STAGES * STAGE;
   static constexpr int ELEMS = O_E + (TTI ? 3 * PE : 0);
   static constexpr int BYTES = ELEMS * (int)sizeof(T);
   // transaction bytes of all boxes of one tile
@@ -59,11 +68,16 @@ struct TmaLayout {
   static constexpr bool FITS = BYTES <= kSmemLimit;
 };
 
-// Tile height: 16 rows when the staged operands fit, else 8.
-template <typename T, int KIND, int NSLS>
+// Layout choice: (PERSIST) two stages of 16-row tiles, else two stages of
+// 8-row tiles; else one stage of 16 or 8 rows (one tile per CTA).
+template <typename T, int KIND, int NSLS, bool PERSIST = true>
 struct TmaPick {
-  static constexpr int TZ = TmaLayout<T, KIND, NSLS, 16>::FITS ? 16 : 8;
-  using Lay = TmaLayout<T, KIND, NSLS, TZ>;
+  static constexpr bool F16x2 = PERSIST && TmaLayout<T, KIND, NSLS, 16, 2>::FITS;
+  static constexpr bool F8x2 = PERSIST && TmaLayout<T, KIND, NSLS, 8, 2>::FITS;
+  static constexpr bool F16x1 = TmaLayout<T, KIND, NSLS, 16, 1>::FITS;
+  static constexpr int TZ = F16x2 ? 16 : (F8x2 ? 8 : (F16x1 ? 16 : 8));
+  static constexpr int STAGES = (F16x2 || F8x2) ? 2 : 1;
+  using Lay = TmaLayout<T, KIND, NSLS, TZ, STAGES>;
   static constexpr bool OK = Lay::FITS;
 };
 
@@ -77,15 +91,15 @@ struct TmaMaps {
 // Tile and box geometry the host needs (tile lists, grid size, tensor-map
 // boxes) for a medium kind, mechanism count and element size.
 struct TmaBoxes {
-  int TX, TZ, HV, HS, HVP, HSP;
+  int TX, TZ, HV, HS, HVP, HSP, STAGES, NT;
   int SWp, SH, VWp, VH, RWp, RH, MX0, MZ0, MW, MH, NM, CW, CH, NC;
   bool ok;
 };
-TmaBoxes tma_boxes(int kind, int nsls, int esize);
+TmaBoxes tma_boxes(int kind, int nsls, int esize, bool persist);
 
 template <typename T>
 int launch_fused_tma(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
-                     const TmaMaps &maps, int ntiles, cudaStream_t st);
+                     const TmaMaps &maps, int ntiles, int nsm, bool persist, cudaStream_t st);
 
 // Encodes a 2D (depth = 1) or 3D tensor map over an x-fastest array.
 int encode_map(CUtensorMap *map, const void *base, int esize, int nx, int nz, long long depth,

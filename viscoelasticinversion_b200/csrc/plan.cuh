@@ -9,6 +9,7 @@
 struct vi_plan {
   vi_config cfg;
   int device = 0;
+  int nsm = 148;  // streaming multiprocessors of the device
   int Lx = 0, Rx = 0, Tz = 0, Bz = 0, wx = 0, hz = 0;
   size_t esize = 4;  // bytes per real
   // device workspace

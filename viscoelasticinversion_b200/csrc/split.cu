@@ -1,0 +1,535 @@
+// split.cu — the step as two in-place kernels per time step (ISO and VTI).
+//
+//   k_split_vel:    v += dt*b*(div sigma + f) on a 64 x 16 tile; the stresses
+//                   of the tile + 4-cell halo are staged by one TMA box per
+//                   plane, the tile's own v and rho come as 128-bit loads.
+//   k_split_stress: SLS stress + memory variables on a 64 x 16 tile; the new
+//                   velocities of the tile + 4-cell halo are staged by TMA,
+//                   every own-cell operand (sigma, M, stiffness, tau) is a
+//                   128-bit load issued before the arithmetic.  Threads on
+//                   the rows below the free surface also write the stress
+//                   images, so no separate mirror pass is needed.
+//
+// Each cell's operands cross HBM once per kernel: 8 planes for the velocity
+// kernel (sigma 3 + v 2 + rho read, v written) and 2 + 2*(3 + 3N) + N_m for
+// the stress kernel — 156 B per point per step for FP32 VTI with 3 SLS
+// against 136 B for a single fused pass, but with a fraction of the fused
+// kernel's arithmetic per byte, so both kernels run near the HBM roofline.
+// In place is safe: the velocity kernel reads v only at its own cells and
+// never writes sigma; the stress kernel reads v and writes sigma, M and psi
+// only at its own cells.  (TTI needs neighbours' effective rates and stays
+// on the fused ping-pong kernel.)
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "fused_tma.cuh"
+#include "plan.cuh"
+#include "split.cuh"
+#include "tma.cuh"
+
+namespace vb {
+
+namespace {
+
+template <typename T>
+struct Q4 {
+  T v[4];
+};
+__device__ __forceinline__ Q4<float> lds4(const float *p) {
+  const float4 q = *reinterpret_cast<const float4 *>(p);
+  return {{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ Q4<double> lds4(const double *p) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0];
+  const double2 b = reinterpret_cast<const double2 *>(p)[1];
+  return {{a.x, a.y, b.x, b.y}};
+}
+// read-only global 128-bit loads (non-coherent path)
+__device__ __forceinline__ Q4<float> ldg4(const float *p) {
+  const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
+  return {{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ Q4<double> ldg4(const double *p) {
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  return {{a.x, a.y, b.x, b.y}};
+}
+// coherent 128-bit loads of state this kernel also writes (own cells only)
+__device__ __forceinline__ Q4<float> ldc4(const float *p) {
+  const float4 q = *reinterpret_cast<const float4 *>(p);
+  return {{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ Q4<double> ldc4(const double *p) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0];
+  const double2 b = reinterpret_cast<const double2 *>(p)[1];
+  return {{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void stg4(float *p, const Q4<float> &q) {
+  *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
+}
+__device__ __forceinline__ void stg4(double *p, const Q4<double> &q) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(q.v[0], q.v[1]);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(q.v[2], q.v[3]);
+}
+__device__ __forceinline__ float two_over_s(float s) { return 2.0f * __frcp_rn(s); }
+__device__ __forceinline__ double two_over_s(double s) { return 2.0 / s; }
+
+template <typename T>
+__device__ __forceinline__ void row12s(const T *p, T (&o)[12]) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const Q4<T> v = lds4(p + 4 * q);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[4 * q + k] = v.v[k];
+  }
+}
+template <typename T>
+__device__ __forceinline__ T dps(const T (&u)[12], int c, const T *D) {  // ddxp form
+  return D[0] * (u[c + 1] - u[c]) + D[1] * (u[c + 2] - u[c - 1]) + D[2] * (u[c + 3] - u[c - 2]) +
+         D[3] * (u[c + 4] - u[c - 3]);
+}
+template <typename T>
+__device__ __forceinline__ T dms(const T (&u)[12], int c, const T *D) {  // ddxm form
+  return D[0] * (u[c] - u[c - 1]) + D[1] * (u[c + 1] - u[c - 2]) + D[2] * (u[c + 2] - u[c - 3]) +
+         D[3] * (u[c + 3] - u[c - 4]);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- velocity
+template <typename T>
+__global__ void __launch_bounds__(SplitGeom<T>::NT)
+    k_split_vel(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
+  using G = SplitGeom<T>;
+  constexpr int TX = G::TX, TZ = G::TZ, SW = G::BW, PB = G::PB;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
+  T *s_sxx = reinterpret_cast<T *>(smem_raw) + G::O0;
+  T *s_szz = s_sxx + PB, *s_sxz = s_szz + PB;
+  const int tile = blockIdx.x;
+  const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
+  const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
+  const int tid = threadIdx.x;
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(bar, 3 * G::BOX_BYTES);
+    tma_load_2d(s_sxx, &maps.a, x0 - 4, z0 - 4, bar);
+    tma_load_2d(s_szz, &maps.b, x0 - 4, z0 - 4, bar);
+    tma_load_2d(s_sxz, &maps.c, x0 - 4, z0 - 4, bar);
+  }
+  // own-cell operands while the box lands
+  const int r = tid / (TX / 4), lx = 4 * (tid % (TX / 4));
+  const int gi0 = x0 + lx, gj = z0 + r;
+  const bool act = gi0 < xe && gj < ze;
+  const long long g = (long long)gj * nx + gi0;
+  Q4<T> vxi{}, vzi{}, r0{}, r1{};
+  T r4 = 0;
+  if (act) {
+    vxi = ldc4(a.vx + g);
+    vzi = ldc4(a.vz + g);
+    r0 = ldg4(a.rho + g);
+    r1 = ldg4(a.rho + g + nx);
+    r4 = __ldg(a.rho + g + 4);
+  }
+  const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
+  const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicExch(x.err, 1);
+      mbar_wait_bounded(bar, 0, 1u << 22);
+    }
+    return;
+  }
+  Q4<T> vxn = vxi, vzn = vzi;
+  if (act) {
+    const int sb = (r + 4) * SW + lx;  // box row of the cells; the cells sit at box column lx+4
+    T hxx[12], hxz[12];
+    row12s(s_sxx + sb, hxx);
+    row12s(s_sxz + sb, hxz);
+    T zxz[4] = {0, 0, 0, 0}, zzz[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int q = -4; q <= 4; ++q) {
+      if (q <= 3) {  // ddzm(sxz)
+        const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
+        const Q4<T> v = q == 0 ? Q4<T>{{hxz[4], hxz[5], hxz[6], hxz[7]}} : lds4(s_sxz + sb + q * SW + 4);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) zxz[k] += cq * v.v[k];
+      }
+      if (q >= -3) {  // ddzp(szz)
+        const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
+        const Q4<T> v = lds4(s_szz + sb + q * SW + 4);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) zzz[k] += cq * v.v[k];
+      }
+    }
+    const int zs = strip_z(gj, nz, a.Tz, a.Bz);
+    const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int gi = gi0 + k;
+      T dxx = dps(hxx, 4 + k, a.Dx), dxxz = dms(hxz, 4 + k, a.Dx);
+      T dzxz = zxz[k], dzz = zzz[k];
+      if (xstrip) {
+        const int xs = strip_x(gi, nx, a.Lx, a.Rx);
+        if (xs >= 0) {
+          const T *tb = a.tx;
+          const long long o = (long long)gj * a.wx + xs;
+          T *p0 = a.psix + PX_SXX * a.psix_plane + o, *p1 = a.psix + PX_SXZ * a.psix_plane + o;
+          *p0 = tb[T_BH * nx + gi] * *p0 + tb[T_AH * nx + gi] * dxx;
+          *p1 = tb[T_B * nx + gi] * *p1 + tb[T_A * nx + gi] * dxxz;
+          dxx = dxx * tb[T_IKH * nx + gi] + *p0;
+          dxxz = dxxz * tb[T_IK * nx + gi] + *p1;
+        }
+      }
+      if (zs >= 0) {
+        const T *tb = a.tz;
+        const long long o = (long long)zs * nx + gi;
+        T *p0 = a.psiz + PZ_SXZ * a.psiz_plane + o, *p1 = a.psiz + PZ_SZZ * a.psiz_plane + o;
+        *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * dzxz;
+        *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * dzz;
+        dzxz = dzxz * tb[T_IK * nz + gj] + *p0;
+        dzz = dzz * tb[T_IKH * nz + gj] + *p1;
+      }
+      const T rx = k < 3 ? r0.v[k + 1] : r4;
+      vxn.v[k] = vxi.v[k] + a.dt * two_over_s(r0.v[k] + rx) * (dxx + dzxz);
+      vzn.v[k] = vzi.v[k] + a.dt * two_over_s(r0.v[k] + r1.v[k]) * (dxxz + dzz);
+    }
+    // force sources of this tile (few; each at most once per thread's group)
+    for (int e = e0; e < e1; ++e) {
+      const int4 en = x.tile_ent[e];
+      if ((en.w != TL_FORCE_X && en.w != TL_FORCE_Z) || en.y != gj || en.x < gi0 || en.x >= gi0 + 4)
+        continue;
+      const int k = en.x - gi0;
+      const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
+      const T f = x.amp[en.z] * w;
+      if (en.w == TL_FORCE_X)
+        vxn.v[k] += a.dt * two_over_s(r0.v[k] + (k < 3 ? r0.v[k + 1] : r4)) * f;
+      else
+        vzn.v[k] += a.dt * two_over_s(r0.v[k] + r1.v[k]) * f;
+    }
+    stg4(a.vx + g, vxn);
+    stg4(a.vz + g, vzn);
+    if (x.traces && x.it < x.tnt) {
+      for (int e = e0; e < e1; ++e) {
+        const int4 en = x.tile_ent[e];
+        if (en.w != TL_RECEIVER || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
+        x.traces[(long long)en.z * x.tnt + x.it] = vxn.v[en.x - gi0];
+        x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = vzn.v[en.x - gi0];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ stress
+template <typename T, int KIND, int NSLS>
+__global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 2 : 1)
+    k_split_stress(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
+  using G = SplitGeom<T>;
+  constexpr int TX = G::TX, TZ = G::TZ, SW = G::BW, PB = G::PB;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
+  T *s_vx = reinterpret_cast<T *>(smem_raw) + G::O0;
+  T *s_vz = s_vx + PB;
+  const int tile = blockIdx.x;
+  const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
+  const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
+  const int tid = threadIdx.x;
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(bar, 2 * G::BOX_BYTES);
+    tma_load_2d(s_vx, &maps.a, x0 - 4, z0 - 4, bar);
+    tma_load_2d(s_vz, &maps.b, x0 - 4, z0 - 4, bar);
+  }
+  const int r = tid / (TX / 4), lx = 4 * (tid % (TX / 4));
+  const int gi0 = x0 + lx, gj = z0 + r;
+  const bool act = gi0 < xe && gj < ze;
+  const long long g = (long long)gj * nx + gi0;
+  // every own-cell operand, issued before the arithmetic
+  Q4<T> sxx{}, szz{}, sxz{}, c13{}, c55a{}, c55b{}, c11{}, c33{}, tau{};
+  T c55a4 = 0, c55b4 = 0;
+  Q4<T> m[3 * (NSLS > 0 ? NSLS : 1)];
+  if (act) {
+    sxx = ldc4(a.sxx + g);
+    szz = ldc4(a.szz + g);
+    sxz = ldc4(a.sxz + g);
+    c13 = ldg4(a.c13 + g);
+    c55a = ldg4(a.c55 + g);
+    c55b = ldg4(a.c55 + g + nx);
+    c55a4 = __ldg(a.c55 + g + 4);
+    c55b4 = __ldg(a.c55 + g + nx + 4);
+    if constexpr (KIND != VI_MEDIUM_ISO) {
+      c11 = ldg4(a.c11 + g);
+      c33 = ldg4(a.c33 + g);
+    }
+    if constexpr (NSLS > 0) {
+      tau = ldg4(a.tau + g);
+#pragma unroll
+      for (int q = 0; q < 3 * NSLS; ++q) m[q] = ldc4(a.m + q * a.mstride + g);
+    }
+  }
+  const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
+  const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicExch(x.err, 1);
+      mbar_wait_bounded(bar, 0, 1u << 22);
+    }
+    return;
+  }
+  if (!act) return;
+  // ---- strain rates from the staged velocities (cells at box column lx+4)
+  const int vb = (r + 4) * SW + lx;
+  T hvx[12], hvz[12];
+  row12s(s_vx + vb, hvx);
+  row12s(s_vz + vb, hvz);
+  T zvz[4] = {0, 0, 0, 0}, zvx[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int q = -4; q <= 4; ++q) {
+    if (q <= 3) {  // ddzm(vz)
+      const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
+      const Q4<T> v = q == 0 ? Q4<T>{{hvz[4], hvz[5], hvz[6], hvz[7]}} : lds4(s_vz + vb + q * SW + 4);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) zvz[k] += cq * v.v[k];
+    }
+    if (q >= -3) {  // ddzp(vx)
+      const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
+      const Q4<T> v = q == 0 ? Q4<T>{{hvx[4], hvx[5], hvx[6], hvx[7]}} : lds4(s_vx + vb + q * SW + 4);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) zvx[k] += cq * v.v[k];
+    }
+  }
+  const int zs = strip_z(gj, nz, a.Tz, a.Bz);
+  const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
+  const bool surf = x.fs && gj == L;
+  T rxx[4], rzz[4], rxz[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int gi = gi0 + k;
+    T dxvx = dms(hvx, 4 + k, a.Dx), dxvz = dps(hvz, 4 + k, a.Dx);
+    T dzvz = zvz[k], dzvx = zvx[k];
+    if (xstrip) {
+      const int xs = strip_x(gi, nx, a.Lx, a.Rx);
+      if (xs >= 0) {
+        const T *tb = a.tx;
+        const long long o = (long long)gj * a.wx + xs;
+        T *p0 = a.psix + PX_VX * a.psix_plane + o, *p1 = a.psix + PX_VZ * a.psix_plane + o;
+        *p0 = tb[T_B * nx + gi] * *p0 + tb[T_A * nx + gi] * dxvx;
+        *p1 = tb[T_BH * nx + gi] * *p1 + tb[T_AH * nx + gi] * dxvz;
+        dxvx = dxvx * tb[T_IK * nx + gi] + *p0;
+        dxvz = dxvz * tb[T_IKH * nx + gi] + *p1;
+      }
+    }
+    if (zs >= 0) {
+      const T *tb = a.tz;
+      const long long o = (long long)zs * nx + gi;
+      T *p0 = a.psiz + PZ_VZ * a.psiz_plane + o, *p1 = a.psiz + PZ_VX * a.psiz_plane + o;
+      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * dzvz;
+      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * dzvx;
+      dzvz = dzvz * tb[T_IK * nz + gj] + *p0;
+      dzvx = dzvx * tb[T_IKH * nz + gj] + *p1;
+    }
+    rxx[k] = dxvx;
+    rzz[k] = dzvz;
+    rxz[k] = dzvx + dxvz;
+  }
+  // ---- SLS effective rates and the stress update
+  const T dt = a.dt;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    T exx = rxx[k], ezz = rzz[k], exz = rxz[k];
+    if constexpr (NSLS > 0) {
+      T Sxx = 0, Szz = 0, Sxz = 0;
+#pragma unroll
+      for (int n = 0; n < NSLS; ++n) {
+        Sxx += m[0 * NSLS + n].v[k];
+        Szz += m[1 * NSLS + n].v[k];
+        Sxz += m[2 * NSLS + n].v[k];
+      }
+      const T t = tau.v[k], t1 = T(1) + t;
+      exx = t1 * rxx[k] + t * Sxx;
+      ezz = t1 * rzz[k] + t * Szz;
+      exz = t1 * rxz[k] + t * Sxz;
+    }
+    const T C13 = c13.v[k];
+    const T C11 = KIND == VI_MEDIUM_ISO ? C13 + T(2) * c55a.v[k] : c11.v[k];
+    const T C33 = KIND == VI_MEDIUM_ISO ? C11 : c33.v[k];
+    if (surf) ezz = -(C13 * exx) / C33;
+    const T c55r = k < 3 ? c55a.v[k + 1] : c55a4, c55br = k < 3 ? c55b.v[k + 1] : c55b4;
+    const T C55h = T(0.25) * (c55a.v[k] + c55r + c55b.v[k] + c55br);
+    sxx.v[k] += dt * (C11 * exx + C13 * ezz);
+    szz.v[k] += dt * (C13 * exx + C33 * ezz);
+    sxz.v[k] += dt * (C55h * exz);
+  }
+  if constexpr (NSLS > 0) {
+#pragma unroll
+    for (int n = 0; n < NSLS; ++n) {
+      const T a1 = a.a1[n], a2 = a.a2[n];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        m[0 * NSLS + n].v[k] += dt * (a1 * rxx[k] + a2 * m[0 * NSLS + n].v[k]);
+        m[1 * NSLS + n].v[k] =
+            surf ? T(0) : m[1 * NSLS + n].v[k] + dt * (a1 * rzz[k] + a2 * m[1 * NSLS + n].v[k]);
+        m[2 * NSLS + n].v[k] += dt * (a1 * rxz[k] + a2 * m[2 * NSLS + n].v[k]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 3 * NSLS; ++q) stg4(a.m + q * a.mstride + g, m[q]);
+  }
+  for (int e = e0; e < e1; ++e) {
+    const int4 en = x.tile_ent[e];
+    if (en.w != TL_EXPLOSIVE || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
+    const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
+    sxx.v[en.x - gi0] += dt * x.amp[en.z] * w;
+    szz.v[en.x - gi0] += dt * x.amp[en.z] * w;
+  }
+  if (surf) szz = Q4<T>{{0, 0, 0, 0}};
+  stg4(a.sxx + g, sxx);
+  stg4(a.szz + g, szz);
+  stg4(a.sxz + g, sxz);
+  if (x.fs) {
+    // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
+    const int k = gj - L;
+    if (k >= 1 && k <= L) {
+      Q4<T> im;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) im.v[q] = -szz.v[q];
+      stg4(a.szz + (long long)(L - k) * nx + gi0, im);
+    }
+    if (k >= 0 && k < L) {
+      Q4<T> im;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) im.v[q] = -sxz.v[q];
+      stg4(a.sxz + (long long)(L - 1 - k) * nx + gi0, im);
+    }
+  }
+}
+
+// ------------------------------------------------------------------- host
+template <typename T, int KIND, int NSLS>
+static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                         int ntiles, cudaStream_t st) {
+  using G = SplitGeom<T>;
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set & (1ULL << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_STRESS);
+    if (e != cudaSuccess) return cuda_check(e, "split stress smem attribute");
+    attr_set |= 1ULL << dev;
+  }
+  k_split_stress<T, KIND, NSLS><<<ntiles, G::NT, G::SMEM_STRESS, st>>>(a, x, m);
+  return VI_OK;
+}
+
+template <typename T>
+int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
+                     cudaStream_t st) {
+  using G = SplitGeom<T>;
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set & (1ULL << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(k_split_vel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         G::SMEM_VEL);
+    if (e != cudaSuccess) return cuda_check(e, "split velocity smem attribute");
+    attr_set |= 1ULL << dev;
+  }
+  k_split_vel<T><<<ntiles, G::NT, G::SMEM_VEL, st>>>(a, x, m);
+  return VI_OK;
+}
+
+template <typename T>
+int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
+                        const SplitMaps &m, int ntiles, cudaStream_t st) {
+#define VB_CASE(K, N) \
+  if (kind == K && a.nsls == N) return launch_stress<T, K, N>(a, x, m, ntiles, st);
+#define VB_KIND(K) VB_CASE(K, 0) VB_CASE(K, 1) VB_CASE(K, 2) VB_CASE(K, 3) VB_CASE(K, 4) VB_CASE(K, 5)
+  VB_KIND(VI_MEDIUM_ISO)
+  VB_KIND(VI_MEDIUM_VTI)
+#undef VB_KIND
+#undef VB_CASE
+  return set_error(VI_ERR_ARG, "the split step covers ISO and VTI media");
+}
+
+static bool al16(const void *q) { return ((uintptr_t)q & 15) == 0; }
+
+template <typename T>
+bool split_eligible(const vi_plan *p, const StepArgs<T> &a) {
+  const vi_config &c = p->cfg;
+  if (c.medium == VI_MEDIUM_TTI || c.nx % 4 != 0) return false;
+  if (((size_t)c.nx * sizeof(T)) % 16 != 0) return false;
+  const void *ptrs[] = {a.vx, a.vz, a.sxx, a.szz, a.sxz, a.rho, a.c11, a.c13, a.c33, a.c55, a.tau, a.m};
+  for (const void *q : ptrs)
+    if (q && !al16(q)) return false;
+  if (c.nsls > 0 && ((size_t)a.mstride * sizeof(T)) % 16 != 0) return false;
+  return true;
+}
+
+template <typename T>
+int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st) {
+  using G = SplitGeom<T>;
+  const vi_config &c = p->cfg;
+  if (!split_eligible<T>(p, a))
+    return set_error(VI_ERR_ARG, "split step needs an ISO/VTI medium, nx % 4 == 0 and 16-byte aligned planes");
+  if (nsteps == 0) return VI_OK;
+  int ntx, ntz;
+  std::vector<int> off;
+  std::vector<int4> ent;
+  build_tile_lists(c.nx, c.nz, G::TX, G::TZ, 0, s, off, ent, ntx, ntz);
+  int *d_off = nullptr;
+  int4 *d_ent = nullptr;
+  int rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent);
+  if (rc) return rc;
+  const int e = sizeof(T);
+  SplitMaps mv, ms;
+  if ((rc = encode_map(&mv.a, a.sxx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+  if ((rc = encode_map(&mv.b, a.szz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+  if ((rc = encode_map(&mv.c, a.sxz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+  if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+  if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+  ms.c = ms.b;
+  FusedExtras<T> x;
+  x.ntx = ntx;
+  x.fs = c.free_surface;
+  x.tile_off = d_off;
+  x.tile_ent = d_ent;
+  x.amp = (const T *)p->damp;
+  x.wavelet = (s && s->nsrc) ? (const T *)s->wavelet_dev : nullptr;
+  x.wnt = (s && s->nsrc) ? s->wavelet_nt : 0;
+  x.traces = (s && s->nrec) ? (T *)s->traces_dev : nullptr;
+  x.tnt = (s && s->nrec) ? s->traces_nt : 0;
+  x.nrec = s ? s->nrec : 0;
+  x.err = (int *)p->errflag;
+  // in place on the current psi set
+  const int cur = p->psi_cur;
+  if (a.psix) a.psix = a.psix_o = (T *)p->psix + cur * kPsiPerSet * p->psix_plane;
+  if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
+  const int ntiles = ntx * ntz;
+  for (int k = 0; k < nsteps; ++k) {
+    x.it = it0 + k;
+    if ((rc = launch_split_vel<T>(a, x, mv, ntiles, st))) return rc;
+    if ((rc = launch_split_stress<T>(c.medium, a, x, ms, ntiles, st))) return rc;
+  }
+  return VI_OK;
+}
+
+template bool split_eligible<float>(const vi_plan *, const StepArgs<float> &);
+template bool split_eligible<double>(const vi_plan *, const StepArgs<double> &);
+template int split_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t);
+template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int, cudaStream_t);
+
+template int launch_split_vel<float>(const StepArgs<float> &, const FusedExtras<float> &,
+                                     const SplitMaps &, int, cudaStream_t);
+template int launch_split_vel<double>(const StepArgs<double> &, const FusedExtras<double> &,
+                                      const SplitMaps &, int, cudaStream_t);
+template int launch_split_stress<float>(int, const StepArgs<float> &, const FusedExtras<float> &,
+                                        const SplitMaps &, int, cudaStream_t);
+template int launch_split_stress<double>(int, const StepArgs<double> &, const FusedExtras<double> &,
+                                         const SplitMaps &, int, cudaStream_t);
+
+}  // namespace vb

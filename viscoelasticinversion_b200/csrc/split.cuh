@@ -1,0 +1,49 @@
+// split.cuh — geometry and host interface of the two-kernel (velocity,
+// stress) in-place step for ISO and VTI media.
+#pragma once
+
+#include <cuda.h>
+
+#include "common.cuh"
+#include "fused.cuh"
+
+struct vi_plan;
+
+namespace vb {
+
+template <typename T>
+struct SplitGeom {
+  static constexpr int TX = 64, TZ = 16, NT = 256;  // one 4-cell group per thread
+  static constexpr int BW = TX + 8, BH = TZ + 8;    // staged box: tile + 4-cell halo
+  static constexpr int PB =
+      (int)(((long long)BW * BH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
+  static constexpr int O0 = 128 / (int)sizeof(T);  // after the barrier slot
+  static constexpr int BOX_BYTES = BW * BH * (int)sizeof(T);
+  static constexpr int SMEM_VEL = 128 + 3 * PB * (int)sizeof(T);
+  static constexpr int SMEM_STRESS = 128 + 2 * PB * (int)sizeof(T);
+};
+
+// TMA maps of the staged planes: (sxx, szz, sxz) for the velocity kernel,
+// (vx, vz) for the stress kernel.
+struct SplitMaps {
+  CUtensorMap a, b, c;
+};
+
+template <typename T>
+int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
+                     cudaStream_t st);
+template <typename T>
+int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
+                        const SplitMaps &m, int ntiles, cudaStream_t st);
+
+// Runs nsteps split steps in place on the caller's fields.  Returns
+// VI_ERR_ARG (without side effects) when the configuration is not eligible
+// (TTI, nx % 4 != 0 or unaligned planes).
+template <typename T>
+int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st);
+
+// true when split_steps can run this plan and these pointers
+template <typename T>
+bool split_eligible(const vi_plan *p, const StepArgs<T> &a);
+
+}  // namespace vb
