@@ -151,7 +151,8 @@ int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
  * trap; this is how a device-side failure reaches the caller. */
 int vi_plan_status(vi_plan *plan, void *stream);
 /* Which kernel the last vi_step ran: 1 plain, 2 fused, 3 fused TMA-staged,
- * 4 fused TMA-staged single-stage, 5 split velocity/stress pair. */
+ * 4 fused TMA-staged single-stage, 5 split velocity/stress pair, 6 split
+ * pair, persistent and TMA-pipelined. */
 int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
 
 /* ---- time stepping ------------------------------------------------------ */
@@ -164,13 +165,14 @@ int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
  * with _vel_1Q! (:3-20), _stress_1Q! (:59-85), the free-surface kernels
  * (free-surface-kernels.jl:16-213) and the CPML/ψ recursion
  * (sciml_solver/CPML.jl:291-328).  `shot` may be NULL (no sources or
- * receivers).  kernel_variant: 0 = default (the split pair for ISO/VTI when
- * nx % 4 == 0 and every plane is 16-byte aligned; else the TMA-staged fused
- * kernel when eligible; else the fused kernel), 1 = plain multi-kernel path
- * (in place), 2 = fused kernel without TMA, 3 = TMA-staged fused kernel
- * (persistent, two stages when they fit), 4 = TMA-staged fused kernel with
- * one stage, 5 = split velocity/stress kernel pair (in place; VI_ERR_ARG
- * when not eligible).  Variants 3-5 return VI_ERR_ARG when not eligible. */
+ * receivers).  kernel_variant: 0 = default (for ISO/VTI with nx % 4 == 0
+ * and 16-byte aligned planes the split pair, else the TMA-staged
+ * fused kernel when eligible, else the fused kernel), 1 = plain
+ * multi-kernel path (in place), 2 = fused kernel without TMA, 3 = TMA-staged
+ * fused kernel (persistent, two stages when they fit), 4 = TMA-staged fused
+ * kernel with one stage, 5 = split velocity/stress kernel pair (in place,
+ * one tile per CTA), 6 = the split pair as persistent TMA-pipelined kernels.
+ * Variants 3-6 return VI_ERR_ARG when not eligible. */
 int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);

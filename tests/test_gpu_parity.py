@@ -38,18 +38,18 @@ def oracle_run(oracle_lib, name):
     return _cache[name]
 
 
-KERNEL_OF_VARIANT = {1: "plain", 2: "fused", 3: "fused-tma", 4: "fused-tma-1stage", 5: "split"}
+KERNEL_OF_VARIANT = {1: "plain", 2: "fused", 3: "fused-tma", 4: "fused-tma-1stage", 5: "split", 6: "split-pipelined"}
 
 
 @pytest.mark.parametrize("name", ["iso256", "vti256x128", "tti256x128", "iso-odd37x29"])
 @pytest.mark.parametrize("precision", ["f32", "f64"])
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
 def test_parity_with_oracle(oracle_lib, name, precision, variant):
     w, tr_ref, st_ref = oracle_run(oracle_lib, name)
     assert np.abs(tr_ref).max() > 0
     from viscoelasticinversion_b200 import ViError
 
-    if variant in (3, 4, 5) and w.nx % 4 or variant == 5 and w.kind == "tti":
+    if variant in (3, 4, 5, 6) and w.nx % 4 or variant in (5, 6) and w.kind == "tti":
         # not eligible: the explicit variant refuses, the default falls back
         with pytest.raises(ViError):
             run_gpu(w, precision, variant)
@@ -92,7 +92,7 @@ def test_no_free_surface_with_top_cpml_and_force_sources(oracle_lib, kind):
     w.sources = [(80, 60, 1, 1.0), (81, 59, 2, -0.5), (40, 30, 0, 2.0), (80, 60, 2, 0.25)]
     w.wavelets = np.stack([w.wavelets[0]] * 4)
     tr_ref, st_ref = oracle_lib.run(w, precision="f64")
-    for variant in (1, 2, 3, 4) + ((5,) if kind != "tti" else ()):
+    for variant in (1, 2, 3, 4) + ((5, 6) if kind != "tti" else ()):
         tr, st = run_gpu(w, "f64", variant)
         err = compare(tr, st, tr_ref, st_ref, w.nsls)
         assert max(err.values()) < 1e-10, (variant, err)
@@ -154,9 +154,10 @@ def test_full_size_vti_first_steps_match_oracle(oracle_lib):
     w = media.layered()  # 2048 x 1024, dt 0.4 ms, VTI, 3 SLS, 40-cell CPML
     n = 160
     tr_ref, st_ref = oracle_lib.run(w, n, precision="f64")
-    tr, st = run_gpu(w, "f32", 2, nt=n)
-    err = compare(tr, st, tr_ref[:, :, :n], st_ref, w.nsls)
-    assert max(err.values()) < 1e-5, err
+    for variant in (0, 3):  # the default (pipelined split pair) and the fused TMA kernel
+        tr, st = run_gpu(w, "f32", variant, nt=n)
+        err = compare(tr, st, tr_ref[:, :, :n], st_ref, w.nsls)
+        assert max(err.values()) < 1e-5, (variant, err)
 
 
 def test_full_size_vti_linearity_and_paths_agree():
@@ -164,11 +165,12 @@ def test_full_size_vti_linearity_and_paths_agree():
     the response is linear in the source amplitude and the fused and plain
     kernels agree."""
     w = media.layered()
-    tr1, _ = run_gpu(w, "f32", 2)
+    tr1, _ = run_gpu(w, "f32", 0)
     assert np.isfinite(tr1).all() and np.abs(tr1).max() > 0
     w2 = media.layered()
     w2.sources = [(i, j, k, 2.0 * a) for (i, j, k, a) in w2.sources]
-    tr2, _ = run_gpu(w2, "f32", 2)
+    tr2, _ = run_gpu(w2, "f32", 0)
     assert rel_l2(tr2, 2.0 * tr1) < 1e-6
-    tr3, _ = run_gpu(w, "f32", 1)
-    assert rel_l2(tr3, tr1) < 1e-5
+    for variant in (1, 3):  # plain and fused TMA kernels agree with the default
+        tr3, _ = run_gpu(w, "f32", variant)
+        assert rel_l2(tr3, tr1) < 1e-5, variant

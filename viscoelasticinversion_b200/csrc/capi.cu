@@ -280,7 +280,7 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   rc = check_fields(p, f);
   if (rc) return rc;
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
-  if (variant < 0 || variant > 5) return set_error(VI_ERR_ARG, "unknown kernel variant");
+  if (variant < 0 || variant > 6) return set_error(VI_ERR_ARG, "unknown kernel variant");
   if (s && s->nrec > 0 && s->traces_nt > 0 && !s->traces_dev)
     return set_error(VI_ERR_ARG, "receivers need traces_dev");
   rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
@@ -318,10 +318,13 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     if (a.psix) a.psix = a.psix_o = (T *)p->psix + cur * kPsiPerSet * p->psix_plane;
     if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
     for (int k = 0; k < nsteps; ++k) plain_step<T>(a, x, p->cfg.medium, it0 + k, st);
-  } else if (variant == 5 || (variant == 0 && split_eligible<T>(p, a))) {
-    rc = split_steps<T>(p, a, s, it0, nsteps, st);
+  } else if (variant == 5 || variant == 6 || (variant == 0 && split_eligible<T>(p, a))) {
+    // the one-tile-per-CTA pair measures faster than the pipelined pair on
+    // B200 (2048 x 1024 VTI: 27.6 vs 24.4 Gpt/s), so it is the default
+    const bool pipe = variant == 6;
+    rc = split_steps<T>(p, a, s, it0, nsteps, st, pipe);
     if (rc) return rc;
-    p->last_kernel = 5;
+    p->last_kernel = pipe ? 6 : 5;
   } else {
     rc = fused_steps<T>(p, a, s, it0, nsteps, st, variant);
     if (rc) return rc;

@@ -28,75 +28,10 @@
 #include "plan.cuh"
 #include "split.cuh"
 #include "tma.cuh"
+#include "vec.cuh"
 
 namespace vb {
 
-namespace {
-
-template <typename T>
-struct Q4 {
-  T v[4];
-};
-__device__ __forceinline__ Q4<float> lds4(const float *p) {
-  const float4 q = *reinterpret_cast<const float4 *>(p);
-  return {{q.x, q.y, q.z, q.w}};
-}
-__device__ __forceinline__ Q4<double> lds4(const double *p) {
-  const double2 a = reinterpret_cast<const double2 *>(p)[0];
-  const double2 b = reinterpret_cast<const double2 *>(p)[1];
-  return {{a.x, a.y, b.x, b.y}};
-}
-// read-only global 128-bit loads (non-coherent path)
-__device__ __forceinline__ Q4<float> ldg4(const float *p) {
-  const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
-  return {{q.x, q.y, q.z, q.w}};
-}
-__device__ __forceinline__ Q4<double> ldg4(const double *p) {
-  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
-  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
-  return {{a.x, a.y, b.x, b.y}};
-}
-// coherent 128-bit loads of state this kernel also writes (own cells only)
-__device__ __forceinline__ Q4<float> ldc4(const float *p) {
-  const float4 q = *reinterpret_cast<const float4 *>(p);
-  return {{q.x, q.y, q.z, q.w}};
-}
-__device__ __forceinline__ Q4<double> ldc4(const double *p) {
-  const double2 a = reinterpret_cast<const double2 *>(p)[0];
-  const double2 b = reinterpret_cast<const double2 *>(p)[1];
-  return {{a.x, a.y, b.x, b.y}};
-}
-__device__ __forceinline__ void stg4(float *p, const Q4<float> &q) {
-  *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
-}
-__device__ __forceinline__ void stg4(double *p, const Q4<double> &q) {
-  reinterpret_cast<double2 *>(p)[0] = make_double2(q.v[0], q.v[1]);
-  reinterpret_cast<double2 *>(p)[1] = make_double2(q.v[2], q.v[3]);
-}
-__device__ __forceinline__ float two_over_s(float s) { return 2.0f * __frcp_rn(s); }
-__device__ __forceinline__ double two_over_s(double s) { return 2.0 / s; }
-
-template <typename T>
-__device__ __forceinline__ void row12s(const T *p, T (&o)[12]) {
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const Q4<T> v = lds4(p + 4 * q);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) o[4 * q + k] = v.v[k];
-  }
-}
-template <typename T>
-__device__ __forceinline__ T dps(const T (&u)[12], int c, const T *D) {  // ddxp form
-  return D[0] * (u[c + 1] - u[c]) + D[1] * (u[c + 2] - u[c - 1]) + D[2] * (u[c + 3] - u[c - 2]) +
-         D[3] * (u[c + 4] - u[c - 3]);
-}
-template <typename T>
-__device__ __forceinline__ T dms(const T (&u)[12], int c, const T *D) {  // ddxm form
-  return D[0] * (u[c] - u[c - 1]) + D[1] * (u[c + 1] - u[c - 2]) + D[2] * (u[c + 2] - u[c - 3]) +
-         D[3] * (u[c + 3] - u[c - 4]);
-}
-
-}  // namespace
 
 // ---------------------------------------------------------------- velocity
 template <typename T>
@@ -471,28 +406,44 @@ bool split_eligible(const vi_plan *p, const StepArgs<T> &a) {
 }
 
 template <typename T>
-int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st) {
+int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st,
+                bool pipelined) {
   using G = SplitGeom<T>;
   const vi_config &c = p->cfg;
   if (!split_eligible<T>(p, a))
     return set_error(VI_ERR_ARG, "split step needs an ISO/VTI medium, nx % 4 == 0 and 16-byte aligned planes");
+  if (pipelined && !split_p_fits(c.medium, c.nsls, (int)sizeof(T)))
+    return set_error(VI_ERR_ARG, "pipelined split step does not fit shared memory for this medium");
   if (nsteps == 0) return VI_OK;
-  int ntx, ntz;
-  std::vector<int> off;
-  std::vector<int4> ent;
-  build_tile_lists(c.nx, c.nz, G::TX, G::TZ, 0, s, off, ent, ntx, ntz);
+  // per-tile source/receiver lists of the velocity tiling and (pipelined:
+  // its own 64 x 8 tiling) the stress tiling, in one buffer
+  int vtx = G::TX, vtz = G::TZ, stx = G::TX, stz = G::TZ;
+  if (pipelined) split_p_tiles(vtx, vtz, stx, stz);
+  int ntx, ntz, sntx, sntz;
+  std::vector<int> off, soff;
+  std::vector<int4> ent, sent;
+  build_tile_lists(c.nx, c.nz, vtx, vtz, 0, s, off, ent, ntx, ntz);
+  build_tile_lists(c.nx, c.nz, stx, stz, 0, s, soff, sent, sntx, sntz);
+  const int nvoff = (int)off.size();
+  for (int v : soff) off.push_back(v + (int)ent.size());
+  ent.insert(ent.end(), sent.begin(), sent.end());
   int *d_off = nullptr;
   int4 *d_ent = nullptr;
   int rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent);
   if (rc) return rc;
   const int e = sizeof(T);
   SplitMaps mv, ms;
-  if ((rc = encode_map(&mv.a, a.sxx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
-  if ((rc = encode_map(&mv.b, a.szz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
-  if ((rc = encode_map(&mv.c, a.sxz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
-  if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
-  if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
-  ms.c = ms.b;
+  SplitPMaps pv, ps;
+  if (pipelined) {
+    if ((rc = encode_split_p<T>(c, a, pv, ps))) return rc;
+  } else {
+    if ((rc = encode_map(&mv.a, a.sxx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+    if ((rc = encode_map(&mv.b, a.szz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+    if ((rc = encode_map(&mv.c, a.sxz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+    if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+    if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+    ms.c = ms.b;
+  }
   FusedExtras<T> x;
   x.ntx = ntx;
   x.fs = c.free_surface;
@@ -509,19 +460,29 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   const int cur = p->psi_cur;
   if (a.psix) a.psix = a.psix_o = (T *)p->psix + cur * kPsiPerSet * p->psix_plane;
   if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
-  const int ntiles = ntx * ntz;
+  const int ntiles = ntx * ntz, sntiles = sntx * sntz;
+  FusedExtras<T> xs = x;
+  xs.ntx = sntx;
+  xs.tile_off = d_off + nvoff;
   for (int k = 0; k < nsteps; ++k) {
-    x.it = it0 + k;
-    if ((rc = launch_split_vel<T>(a, x, mv, ntiles, st))) return rc;
-    if ((rc = launch_split_stress<T>(c.medium, a, x, ms, ntiles, st))) return rc;
+    x.it = xs.it = it0 + k;
+    if (pipelined) {
+      if ((rc = launch_split_vel_p<T>(a, x, pv, ntiles, p->nsm, st))) return rc;
+      if ((rc = launch_split_stress_p<T>(c.medium, a, xs, ps, sntiles, p->nsm, st))) return rc;
+    } else {
+      if ((rc = launch_split_vel<T>(a, x, mv, ntiles, st))) return rc;
+      if ((rc = launch_split_stress<T>(c.medium, a, xs, ms, sntiles, st))) return rc;
+    }
   }
   return VI_OK;
 }
 
 template bool split_eligible<float>(const vi_plan *, const StepArgs<float> &);
 template bool split_eligible<double>(const vi_plan *, const StepArgs<double> &);
-template int split_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t);
-template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int, cudaStream_t);
+template int split_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t,
+                                bool);
+template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int,
+                                 cudaStream_t, bool);
 
 template int launch_split_vel<float>(const StepArgs<float> &, const FusedExtras<float> &,
                                      const SplitMaps &, int, cudaStream_t);

@@ -36,11 +36,30 @@ template <typename T>
 int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
                         const SplitMaps &m, int ntiles, cudaStream_t st);
 
-// Runs nsteps split steps in place on the caller's fields.  Returns
-// VI_ERR_ARG (without side effects) when the configuration is not eligible
-// (TTI, nx % 4 != 0 or unaligned planes).
+// TMA maps of the pipelined split kernels: velocity (sxx, szz, sxz boxes,
+// vx, vz, rho tiles); stress (vx, vz boxes, sxx, szz, sxz tiles, M, then the
+// coefficient slots and tau).
+struct SplitPMaps {
+  CUtensorMap m[11];
+};
 template <typename T>
-int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st);
+int launch_split_vel_p(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitPMaps &m,
+                       int ntiles, int nsm, cudaStream_t st);
+template <typename T>
+int launch_split_stress_p(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
+                          const SplitPMaps &m, int ntiles, int nsm, cudaStream_t st);
+template <typename T>
+int encode_split_p(const vi_config &c, const StepArgs<T> &a, SplitPMaps &mv, SplitPMaps &ms);
+bool split_p_fits(int kind, int nsls, int esize);
+void split_p_tiles(int &vtx, int &vtz, int &stx, int &stz);
+
+// Runs nsteps split steps in place on the caller's fields, with the
+// one-tile-per-CTA kernels or (pipelined) the persistent TMA-pipelined
+// kernels.  Returns VI_ERR_ARG (without side effects) when the
+// configuration is not eligible (TTI, nx % 4 != 0 or unaligned planes).
+template <typename T>
+int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st,
+                bool pipelined);
 
 // true when split_steps can run this plan and these pointers
 template <typename T>
