@@ -52,6 +52,8 @@ def parse_args():
     p.add_argument("--variant", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--batch-shots", type=int, default=64)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     return p.parse_args()
 
@@ -178,6 +180,81 @@ def run_reference(a):
                          "sample": sample},
         "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def measure_batch(a, dev, stream, max_over_ranks, barrier, world):
+    """Shots/s of the batched TTI gather (64 shots, grids from {512²,
+    1024x512, 1536x768, 2048x1024}, nt in [1500, 4000], one CUDA graph)
+    against the plain path (the same fused TMA kernel, one shot after the
+    other, one launch per step, no graph).  Each rank runs its own gather."""
+    import torch
+
+    from viscoelasticinversion_b200 import StepPlan, media
+    from viscoelasticinversion_b200.batch import ShotBatch
+
+    rank = int(os.environ.get("RANK", "0"))
+    ws = media.shot_gather(a.batch_shots, seed=rank, kind="tti")
+    b = ShotBatch(ws, "f32", device=dev.index)
+    b.run()  # tunes the kernel form, captures the graph, runs once
+    b.reset()
+    form = b.status()
+    variant = 3 if form == "two-stage" else 4
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = max_over_ranks(e0.elapsed_time(e1))
+    b.status()
+    # plain: one shot at a time, one launch per step, no graph
+    plans = [StepPlan.for_workload(w, "f32", device=dev.index) for w in ws]
+    per_class = {}
+    for w, p, med, st, wav, tr in zip(ws, plans, b.media, b.states, b.wavelets, b.traces):
+        for t in st.values():
+            t.zero_()
+        p.reset()
+        p.step(med, st, nsteps=min(w.nt, 20), sources=w.sources, wavelets=wav,
+               receivers=w.receivers, traces=tr, variant=variant)  # warm-up
+    torch.cuda.synchronize()
+    barrier()
+    t_plain = 0.0
+    for w, p, med, st, wav, tr in zip(ws, plans, b.media, b.states, b.wavelets, b.traces):
+        for t in st.values():
+            t.zero_()
+        p.reset()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        p.step(med, st, nsteps=w.nt, sources=w.sources, wavelets=wav, receivers=w.receivers,
+               traces=tr, variant=variant)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ms = s0.elapsed_time(s1)
+        t_plain += ms
+        key = f"{w.nx}x{w.nz}"
+        c = per_class.setdefault(key, {"shots": 0, "plain_ms": 0.0, "point_steps": 0})
+        c["shots"] += 1
+        c["plain_ms"] += ms
+        c["point_steps"] += w.nx * w.nz * w.nt
+    plain_ms = max_over_ranks(t_plain)
+    for p in plans:
+        p.close()
+    pts = b.point_steps()
+    n = len(ws)
+    for c in per_class.values():
+        c["plain_gpts"] = c["point_steps"] / (c["plain_ms"] / 1e3) / 1e9
+    out = {"workload": f"tti-gather-{n}shots-grids512..2048x1024-nt1500..4000-f32",
+           "shots": n * world, "kernel_form": form,
+           "batched_ms": batched_ms, "plain_ms": plain_ms,
+           "batched_shots_per_s": n * world / (batched_ms / 1e3),
+           "plain_shots_per_s": n * world / (plain_ms / 1e3),
+           "speedup": plain_ms / batched_ms,
+           "batched_gpts": world * pts / (batched_ms / 1e3) / 1e9,
+           "plain_gpts": world * pts / (plain_ms / 1e3) / 1e9,
+           "plain_per_grid_class": per_class}
+    b.close()
+    return out
 
 
 def run_ours(a):
@@ -312,6 +389,8 @@ def run_ours(a):
                       "api": "vi_forward_host"}
         out["gpu_launches"] += a.steps * launches_per_step
 
+    if not a.no_batch:
+        out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
     if rank == 0 and world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline(w, a.cpu_seconds)
     if rank == 0:

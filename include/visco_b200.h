@@ -187,6 +187,64 @@ int vi_forward_host(vi_plan *plan, const vi_medium *med_host,
                     int32_t nrec, const vi_receiver *rec, int32_t nt,
                     void *traces_host, vi_fields *final_host);
 
+/* ---- batched shots ---------------------------------------------------- */
+/* Many shots of different grids and step counts advancing together.  The
+ * reference solves one problem per call (ViscoelasticProblem.jl:273-309)
+ * and has no batch; this is the B200 form of running its time step for a
+ * whole shot gather: one launch per time step covers the tiles of every
+ * shot still running, and the sequence of launches is one CUDA graph.
+ * Shots must share the medium kind, precision and nsls, and have nx % 4 == 0. */
+typedef struct vi_batch vi_batch;
+#define VI_BATCH_NO_GRAPH 1  /* launch step by step instead of one CUDA graph */
+#define VI_BATCH_RETUNE 2    /* forget the cached kernel-form choice and retune */
+int vi_batch_create(const vi_config *cfgs, int32_t nshots, vi_batch **out);
+int vi_batch_destroy(vi_batch *batch);
+/* Binds shot i: device medium and fields (borrowed until the batch is
+ * destroyed or the shot re-bound), sources/receivers (host lists copied),
+ * and its step count.  Shots start from the state in their fields. */
+int vi_batch_set_shot(vi_batch *batch, int32_t i, const vi_medium *med_dev,
+                      const vi_fields *fields_dev, const vi_shot *shot, int32_t nt);
+/* Runs every shot to its step count on `stream` (asynchronous).  The first
+ * run (or VI_BATCH_RETUNE) times the kernel forms on the bound shots for a
+ * few steps, keeps the faster one for this problem class, and resets the
+ * shots to rest (fields, memory variables and CPML memory zeroed) before
+ * the run proper.  Every run zeroes the CPML memory first. */
+int vi_batch_run(vi_batch *batch, int32_t flags, void *stream);
+/* Synchronizes, reports the kernel form in use (1 two-stage persistent,
+ * 0 one-stage) and any device-side wait failure (VI_ERR_TIMEOUT). */
+int vi_batch_status(vi_batch *batch, void *stream, int32_t *kernel_form);
+
+/* ---- misfit gradient (discrete adjoint) ------------------------------ */
+/* The reference has no receivers, misfit, adjoint or gradient: its only
+ * gradient path is a printed sketch (examples/energy_natural_gradient_example.jl:252-315)
+ * around an optimizer (EnergyNaturalGradient.jl:239-321) that takes a
+ * grad_fn.  This is that grad_fn for the leapfrog step:
+ *   J = 1/2 sum_{t,r} (d - obs)^2 over the vx and vz traces,
+ * d the traces of an nt-step run from rest with the shot's sources and
+ * receivers, obs_dev the observed traces in the same layout
+ * ([2][nrec][nt], plan precision).  grad_dev (8 planes of nx*nz, FP64) gets
+ * dJ/d(rho, c11, c13, c15, c33, c35, c55, tau) in vi_medium's order; for
+ * ISO media the c13 plane holds dJ/dlambda and the c55 plane dJ/dmu (the
+ * others zero).  ISO and VTI media; TTI returns VI_ERR_ARG.  The adjoint
+ * is the exact transpose of the plain in-place step (kernel variant 1),
+ * with the state checkpointed every checkpoint_every steps (<= 0: ceil
+ * sqrt(nt)) in the plan's workspace.  accumulate != 0 adds into grad_dev
+ * (shots summed), else grad_dev is overwritten.  *misfit_host = J (FP64).
+ * The shot's traces_dev, if given with traces_nt >= nt, receives d.
+ * Synchronous on `stream`. */
+int vi_gradient(vi_plan *plan, const vi_medium *med_dev, const vi_shot *shot, int32_t nt,
+                const void *obs_dev, int32_t checkpoint_every, int32_t accumulate,
+                double *grad_dev, double *misfit_host, void *stream);
+/* Chain rule from grad (as vi_gradient leaves it) to (vp, vs, rho, 1/Q)
+ * planes: out4 = [dJ/dvp, dJ/dvs, dJ/drho at fixed velocities, dJ/d(1/Q)].
+ * vp, vs, rho (and for VTI eps, delta; NULL means 0) are FP64 device
+ * planes of np cells; the stiffnesses follow Models.jl:27-52 (ISO:
+ * lambda = rho (vp^2 - 2 vs^2), mu = rho vs^2; VTI: Thomsen).  tau_scale =
+ * d tau / d(1/Q) = N / Kbar of the Q fit (Models.jl:67). */
+int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const double *vp,
+                         const double *vs, const double *rho, const double *eps,
+                         const double *delta, double tau_scale, double *out4, void *stream);
+
 /* ---- staggered derivatives (diff-funcs.jl:3-32) ----------------------- */
 /* du = D(u) over the update region for one plane (device pointers, plan
  * precision).  op: 0 = ddxp, 1 = ddxm, 2 = ddzp, 3 = ddzm.  h is the grid

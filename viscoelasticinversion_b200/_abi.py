@@ -115,7 +115,22 @@ _SIGNATURES = [
                                   C.POINTER(ViFields)]),
     ("vi_diff", C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                           C.c_int32, C.c_double, C.c_void_p]),
+    ("vi_batch_create", C.c_int, [C.POINTER(ViConfig), C.c_int32, C.POINTER(C.c_void_p)]),
+    ("vi_batch_destroy", C.c_int, [C.c_void_p]),
+    ("vi_batch_set_shot", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ViMedium),
+                                    C.POINTER(ViFields), C.POINTER(ViShot), C.c_int32]),
+    ("vi_batch_run", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    ("vi_batch_status", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    ("vi_gradient", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.POINTER(ViShot), C.c_int32,
+                              C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                              C.POINTER(C.c_double), C.c_void_p]),
+    ("vi_gradient_velocity", C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                       C.c_void_p, C.c_void_p]),
 ]
+
+VI_BATCH_NO_GRAPH = 1
+VI_BATCH_RETUNE = 2
 
 
 def exported_names() -> list[str]:

@@ -1,0 +1,619 @@
+// adjoint.cu — discrete adjoint of the time step and the misfit gradient.
+//
+// J = 1/2 sum_n sum_r |d_n,r - obs_n,r|^2 over the vx and vz traces.  The
+// gradient is the exact transpose of the forward step (plain in-place
+// path, plain.cu), taken stage by stage in reverse:
+//
+//   forward step n:  V (velocity, CPML psi_sigma)  ->  receivers  ->
+//                    S (SLS stress + memory variables, CPML psi_v, free
+//                    surface)  ->  explosive sources  ->  stress images
+//   reverse step n:  images^T -> S^T -> r^T (v += -D^T rbar) -> residual at
+//                    the receivers -> V^T -> d^T (sigma += -D^T dbar)
+//
+// The transpose of ddxp is -ddxm (and of ddzp, -ddzm) over cells whose
+// adjoint is zero outside the update region; each psi recursion
+// psi' = b psi + a d, d~ = d/kappa + psi' transposes to
+// dbar = dbar~/kappa + a (psibar' + dbar~), psibar = b (psibar' + dbar~).
+//
+// Memory: the state (v, sigma, M and the current psi set) is stored every
+// K (default ceil(sqrt(nt))) steps; each segment is recomputed forward into
+// K + 1 state slots and walked backwards.  Wavefields and the adjoint state
+// are in the plan's precision; gradients and the misfit accumulate in FP64,
+// each cell gathering its own terms (no atomics, deterministic).
+//
+// Gradients are with respect to the medium planes (rho, c11, c13, c33,
+// c55, tau) — for ISO c13 = lambda and c55 = mu carry dJ/dlambda and
+// dJ/dmu.  vi_gradient_velocity maps them to (vp, vs, rho, 1/Q).
+#include <cmath>
+#include <vector>
+
+#include "plain.cuh"
+#include "plan.cuh"
+
+namespace vb {
+
+namespace {
+
+template <typename T>
+struct AdjArgs {
+  int nx, nz, nsls, kind, fs;
+  int Lx, Rx, Tz, Bz, wx, hz;
+  T dt;
+  T Dx[4], Dz[4];
+  T a1[VI_MAX_SLS], a2[VI_MAX_SLS];
+  const T *rho, *c11, *c13, *c33, *c55, *tau;
+  const T *tx, *tz;
+  long long np, psix_plane, psiz_plane;
+};
+
+// one state slot: [vx vz sxx szz sxz M(3N)] planes, then one psi set
+// (4 x-strip planes, 4 z-strip planes)
+template <typename T>
+struct Slot {
+  T *base;
+  long long np, px, pz;  // plane sizes
+  int nsls;
+  __host__ __device__ T *vx() const { return base; }
+  __host__ __device__ T *vz() const { return base + np; }
+  __host__ __device__ T *sxx() const { return base + 2 * np; }
+  __host__ __device__ T *szz() const { return base + 3 * np; }
+  __host__ __device__ T *sxz() const { return base + 4 * np; }
+  __host__ __device__ T *m() const { return base + 5 * np; }
+  __host__ __device__ T *psix() const { return base + (5 + 3 * nsls) * np; }
+  __host__ __device__ T *psiz() const { return psix() + 4 * px; }
+  __host__ __device__ static long long size(long long np, long long px, long long pz, int nsls) {
+    return (5 + 3 * nsls) * np + 4 * px + 4 * pz;
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ T tap_p(const T *u, long long c, long long s, const T *D) {  // ddxp/ddzp
+  T v = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) v += D[k] * (u[c + (k + 1) * s] - u[c - k * s]);
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T tap_m(const T *u, long long c, long long s, const T *D) {  // ddxm/ddzm
+  T v = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) v += D[k] * (u[c + k * s] - u[c - (k + 1) * s]);
+  return v;
+}
+// bounds-checked forms for the transposes (u is zero outside its region)
+template <typename T>
+__device__ __forceinline__ T tap_p_b(const T *u, int i, int j, int nx, int nz, int ax, const T *D) {
+  T v = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int a = k + 1, b = -k;
+    const int ia = ax == 0 ? i + a : i, ja = ax == 0 ? j : j + a;
+    const int ib = ax == 0 ? i + b : i, jb = ax == 0 ? j : j + b;
+    const T ua = (ia >= 0 && ia < nx && ja >= 0 && ja < nz) ? u[(long long)ja * nx + ia] : T(0);
+    const T ub = (ib >= 0 && ib < nx && jb >= 0 && jb < nz) ? u[(long long)jb * nx + ib] : T(0);
+    v += D[k] * (ua - ub);
+  }
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T tap_m_b(const T *u, int i, int j, int nx, int nz, int ax, const T *D) {
+  T v = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int a = k, b = -(k + 1);
+    const int ia = ax == 0 ? i + a : i, ja = ax == 0 ? j : j + a;
+    const int ib = ax == 0 ? i + b : i, jb = ax == 0 ? j : j + b;
+    const T ua = (ia >= 0 && ia < nx && ja >= 0 && ja < nz) ? u[(long long)ja * nx + ia] : T(0);
+    const T ub = (ib >= 0 && ib < nx && jb >= 0 && jb < nz) ? u[(long long)jb * nx + ib] : T(0);
+    v += D[k] * (ua - ub);
+  }
+  return v;
+}
+
+// CPML forward at one derivative: returns d~ (and the new psi in *pn)
+template <typename T>
+__device__ __forceinline__ T cpml_fwd(T d, T p0, T a, T b, T ik, T *pn) {
+  const T p = b * p0 + a * d;
+  *pn = p;
+  return d * ik + p;
+}
+
+// ---- images^T: fold the ghost-row adjoints into the rows they mirror ----
+template <typename T>
+__global__ void k_mirror_t(T *sb_zz, T *sb_xz, int nx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx) return;
+#pragma unroll
+  for (int k = 1; k <= L; ++k) {
+    const long long g = (long long)(L - k) * nx + i;
+    sb_zz[(long long)(L + k) * nx + i] -= sb_zz[g];
+    sb_zz[g] = T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < L; ++k) {
+    const long long g = (long long)(L - 1 - k) * nx + i;
+    sb_xz[(long long)(L + k) * nx + i] -= sb_xz[g];
+    sb_xz[g] = T(0);
+  }
+}
+
+// ---- S^T: SLS stress stage transposed, per cell of the update region ----
+// scratch planes: rbar[0..3] = (xx, zz, zx, xz) strain-rate adjoints, q = dt*sxzbar*exz
+template <typename T>
+__global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot<T> x1, Slot<T> ab,
+                                                   T *rbar, T *q, double *gc11, double *gc13,
+                                                   double *gc33, double *gtau) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
+  if (i >= A.nx - L || j >= A.nz - L) return;
+  const int nx = A.nx;
+  const long long c = (long long)j * nx + i, np = A.np;
+  const int N = A.nsls;
+  // forward strain rates from v(n+1) with the psi of step n
+  T r[4];  // xx = ddxm vx, zz = ddzm vz, zx = ddzp vx, xz = ddxp vz
+  r[0] = tap_m(x1.vx(), c, 1, A.Dx);
+  r[1] = tap_m(x1.vz(), c, nx, A.Dz);
+  r[2] = tap_p(x1.vx(), c, nx, A.Dz);
+  r[3] = tap_p(x1.vz(), c, 1, A.Dx);
+  T ik[4] = {1, 1, 1, 1}, ca[4] = {0, 0, 0, 0}, cb[4] = {0, 0, 0, 0};
+  T *pb[4] = {nullptr, nullptr, nullptr, nullptr};
+  const int xs = strip_x(i, nx, A.Lx, A.Rx), zs = strip_z(j, A.nz, A.Tz, A.Bz);
+  if (xs >= 0) {
+    const long long o = (long long)j * A.wx + xs;
+    // x: xx at integer node (PX_VX), xz at half node (PX_VZ)
+    ik[0] = A.tx[T_IK * nx + i]; ca[0] = A.tx[T_A * nx + i]; cb[0] = A.tx[T_B * nx + i];
+    ik[3] = A.tx[T_IKH * nx + i]; ca[3] = A.tx[T_AH * nx + i]; cb[3] = A.tx[T_BH * nx + i];
+    T pn;
+    r[0] = cpml_fwd(r[0], x0.psix()[PX_VX * A.psix_plane + o], ca[0], cb[0], ik[0], &pn);
+    r[3] = cpml_fwd(r[3], x0.psix()[PX_VZ * A.psix_plane + o], ca[3], cb[3], ik[3], &pn);
+    pb[0] = ab.psix() + PX_VX * A.psix_plane + o;
+    pb[3] = ab.psix() + PX_VZ * A.psix_plane + o;
+  }
+  if (zs >= 0) {
+    const int nz = A.nz;
+    const long long o = (long long)zs * nx + i;
+    ik[1] = A.tz[T_IK * nz + j]; ca[1] = A.tz[T_A * nz + j]; cb[1] = A.tz[T_B * nz + j];
+    ik[2] = A.tz[T_IKH * nz + j]; ca[2] = A.tz[T_AH * nz + j]; cb[2] = A.tz[T_BH * nz + j];
+    T pn;
+    r[1] = cpml_fwd(r[1], x0.psiz()[PZ_VZ * A.psiz_plane + o], ca[1], cb[1], ik[1], &pn);
+    r[2] = cpml_fwd(r[2], x0.psiz()[PZ_VX * A.psiz_plane + o], ca[2], cb[2], ik[2], &pn);
+    pb[1] = ab.psiz() + PZ_VZ * A.psiz_plane + o;
+    pb[2] = ab.psiz() + PZ_VX * A.psiz_plane + o;
+  }
+  const T rt[3] = {r[0], r[1], r[2] + r[3]};  // xx, zz, engineering xz
+  T S[3] = {0, 0, 0};
+  for (int n = 0; n < N; ++n)
+    for (int k = 0; k < 3; ++k) S[k] += x0.m()[(k * N + n) * np + c];
+  const T tau = N > 0 ? A.tau[c] : T(0);
+  T e[3];
+  for (int k = 0; k < 3; ++k) e[k] = N > 0 ? (T(1) + tau) * rt[k] + tau * S[k] : rt[k];
+  const T C13 = A.c13[c];
+  const T C11 = A.kind == VI_MEDIUM_ISO ? C13 + T(2) * A.c55[c] : A.c11[c];
+  const T C33 = A.kind == VI_MEDIUM_ISO ? C11 : A.c33[c];
+  const T C55h = T(0.25) * (A.c55[c] + A.c55[c + 1] + A.c55[c + nx] + A.c55[c + nx + 1]);
+  const bool surf = A.fs && j == L;
+  T *sbx = ab.sxx(), *sbz = ab.szz(), *sbq = ab.sxz();
+  const T bxx = sbx[c], bzz = sbz[c], bxz = sbq[c];
+  const T dt = A.dt;
+  T eb[3];
+  if (!surf) {
+    eb[0] = dt * (C11 * bxx + C13 * bzz);
+    eb[1] = dt * (C13 * bxx + C33 * bzz);
+    gc11[c] += (double)dt * bxx * e[0];
+    gc13[c] += (double)dt * (bxx * e[1] + bzz * e[0]);
+    gc33[c] += (double)dt * bzz * e[1];
+  } else {
+    // sxx' = sxx + dt (C11 - C13^2/C33) exx; szz' = 0
+    const T ceff = C11 - C13 * C13 / C33;
+    eb[0] = dt * ceff * bxx;
+    eb[1] = T(0);
+    const double w = (double)dt * bxx * e[0];
+    gc11[c] += w;
+    gc13[c] += w * (-2.0 * (double)C13 / (double)C33);
+    gc33[c] += w * ((double)C13 * C13 / ((double)C33 * C33));
+    sbz[c] = T(0);
+  }
+  eb[2] = dt * C55h * bxz;
+  q[c] = dt * bxz * e[2];
+  if (N > 0) {
+    double gt = 0;
+    for (int k = 0; k < 3; ++k) gt += (double)eb[k] * ((double)rt[k] + S[k]);
+    gtau[c] += gt;
+  }
+  // memory variables and the strain-rate adjoints
+  T rtb[3];
+  for (int k = 0; k < 3; ++k) rtb[k] = (N > 0 ? (T(1) + tau) : T(1)) * eb[k];
+  for (int n = 0; n < N; ++n) {
+    for (int k = 0; k < 3; ++k) {
+      T *mb = ab.m() + (k * N + n) * np + c;
+      const bool dead = surf && k == 1;  // Mzz' = 0 on the surface
+      const T mbo = dead ? T(0) : *mb;
+      rtb[k] += dt * A.a1[n] * mbo;
+      *mb = tau * eb[k] + mbo * (T(1) + dt * A.a2[n]);
+      if (dead) *mb = T(0);
+    }
+  }
+  // psi transposes: rbar = rtbar/kappa + a (psibar' + rtbar), psibar = b (...)
+  T rb[4] = {rtb[0], rtb[1], rtb[2], rtb[2]};
+  for (int k = 0; k < 4; ++k) {
+    if (pb[k]) {
+      const T P = *pb[k] + rb[k];
+      *pb[k] = cb[k] * P;
+      rb[k] = rb[k] * ik[k] + ca[k] * P;
+    }
+    rbar[k * np + c] = rb[k];
+  }
+}
+
+// gc55 gathers the 4 half-node terms that average mu around each cell
+template <typename T>
+__global__ void k_gather_c55(const T *q, double *gc55, int nx, int nz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= nx || j >= nz) return;
+  double s = 0;
+  for (int dj = 0; dj <= 1; ++dj)
+    for (int di = 0; di <= 1; ++di) {
+      const int ii = i - di, jj = j - dj;
+      if (ii >= 0 && jj >= 0) s += q[(long long)jj * nx + ii];
+    }
+  gc55[(long long)j * nx + i] += 0.25 * s;
+}
+
+// v += -D^T rbar over the update region
+template <typename T>
+__global__ void k_rates_t(AdjArgs<T> A, Slot<T> ab, const T *rbar) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
+  if (i >= A.nx - L || j >= A.nz - L) return;
+  const int nx = A.nx, nz = A.nz;
+  const long long c = (long long)j * nx + i, np = A.np;
+  ab.vx()[c] -= tap_p_b(rbar, i, j, nx, nz, 0, A.Dx) + tap_m_b(rbar + 2 * np, i, j, nx, nz, 1, A.Dz);
+  ab.vz()[c] -= tap_p_b(rbar + np, i, j, nx, nz, 1, A.Dz) + tap_m_b(rbar + 3 * np, i, j, nx, nz, 0, A.Dx);
+}
+
+// residual at the receivers of step it: vbar += d - obs
+template <typename T>
+__global__ void k_residual(Slot<T> ab, Slot<T> x1, const int2 *rec, int nrec, const T *obs, int ont,
+                           int it, int nx) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrec) return;
+  const long long c = (long long)rec[r].y * nx + rec[r].x;
+  atomicAdd(ab.vx() + c, x1.vx()[c] - obs[(long long)r * ont + it]);
+  atomicAdd(ab.vz() + c, x1.vz()[c] - obs[(long long)(nrec + r) * ont + it]);
+}
+
+// V^T per cell: dbar (4 planes: sxx-x, sxz-z, sxz-x, szz-z) and the
+// buoyancy-gradient terms h (2 planes)
+template <typename T>
+__global__ void __launch_bounds__(256) k_vel_t(AdjArgs<T> A, Slot<T> x0, Slot<T> ab, T *dbar, T *h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
+  if (i >= A.nx - L || j >= A.nz - L) return;
+  const int nx = A.nx, nz = A.nz;
+  const long long c = (long long)j * nx + i, np = A.np;
+  T d[4];
+  d[0] = tap_p(x0.sxx(), c, 1, A.Dx);   // ddxp sxx   (x, half)
+  d[1] = tap_m(x0.sxz(), c, nx, A.Dz);  // ddzm sxz   (z, integer)
+  d[2] = tap_m(x0.sxz(), c, 1, A.Dx);   // ddxm sxz   (x, integer)
+  d[3] = tap_p(x0.szz(), c, nx, A.Dz);  // ddzp szz   (z, half)
+  T ik[4] = {1, 1, 1, 1}, ca[4] = {0, 0, 0, 0}, cb[4] = {0, 0, 0, 0};
+  T *pb[4] = {nullptr, nullptr, nullptr, nullptr};
+  const int xs = strip_x(i, nx, A.Lx, A.Rx), zs = strip_z(j, nz, A.Tz, A.Bz);
+  T pn;
+  if (xs >= 0) {
+    const long long o = (long long)j * A.wx + xs;
+    ik[0] = A.tx[T_IKH * nx + i]; ca[0] = A.tx[T_AH * nx + i]; cb[0] = A.tx[T_BH * nx + i];
+    ik[2] = A.tx[T_IK * nx + i]; ca[2] = A.tx[T_A * nx + i]; cb[2] = A.tx[T_B * nx + i];
+    d[0] = cpml_fwd(d[0], x0.psix()[PX_SXX * A.psix_plane + o], ca[0], cb[0], ik[0], &pn);
+    d[2] = cpml_fwd(d[2], x0.psix()[PX_SXZ * A.psix_plane + o], ca[2], cb[2], ik[2], &pn);
+    pb[0] = ab.psix() + PX_SXX * A.psix_plane + o;
+    pb[2] = ab.psix() + PX_SXZ * A.psix_plane + o;
+  }
+  if (zs >= 0) {
+    const long long o = (long long)zs * nx + i;
+    ik[1] = A.tz[T_IK * nz + j]; ca[1] = A.tz[T_A * nz + j]; cb[1] = A.tz[T_B * nz + j];
+    ik[3] = A.tz[T_IKH * nz + j]; ca[3] = A.tz[T_AH * nz + j]; cb[3] = A.tz[T_BH * nz + j];
+    d[1] = cpml_fwd(d[1], x0.psiz()[PZ_SXZ * A.psiz_plane + o], ca[1], cb[1], ik[1], &pn);
+    d[3] = cpml_fwd(d[3], x0.psiz()[PZ_SZZ * A.psiz_plane + o], ca[3], cb[3], ik[3], &pn);
+    pb[1] = ab.psiz() + PZ_SXZ * A.psiz_plane + o;
+    pb[3] = ab.psiz() + PZ_SZZ * A.psiz_plane + o;
+  }
+  const T bx = T(2) / (A.rho[c] + A.rho[c + 1]);
+  const T bz = T(2) / (A.rho[c] + A.rho[c + nx]);
+  const T vbx = ab.vx()[c], vbz = ab.vz()[c];
+  // d(vx')/d rho = dt * (-bx^2 / 2) * div
+  h[c] = A.dt * T(-0.5) * bx * bx * (d[0] + d[1]) * vbx;
+  h[np + c] = A.dt * T(-0.5) * bz * bz * (d[2] + d[3]) * vbz;
+  T db[4] = {A.dt * bx * vbx, A.dt * bx * vbx, A.dt * bz * vbz, A.dt * bz * vbz};
+  for (int k = 0; k < 4; ++k) {
+    if (pb[k]) {
+      const T P = *pb[k] + db[k];
+      *pb[k] = cb[k] * P;
+      db[k] = db[k] * ik[k] + ca[k] * P;
+    }
+    dbar[k * np + c] = db[k];
+  }
+}
+
+// force sources: their buoyancy factor also depends on rho
+template <typename T>
+__global__ void k_force_rho_t(AdjArgs<T> A, Slot<T> ab, const int4 *src, const T *amp, int nsrc,
+                              const T *wav, int wnt, int it, T *h) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsrc) return;
+  const int4 s = src[q];
+  if (s.z == VI_SRC_EXPLOSIVE) return;
+  const long long c = (long long)s.y * A.nx + s.x;
+  const T f = it < wnt ? amp[q] * wav[(long long)q * wnt + it] : T(0);
+  if (s.z == VI_SRC_FORCE_X) {
+    const T bx = T(2) / (A.rho[c] + A.rho[c + 1]);
+    atomicAdd(h + c, A.dt * T(-0.5) * bx * bx * f * ab.vx()[c]);
+  } else {
+    const T bz = T(2) / (A.rho[c] + A.rho[c + A.nx]);
+    atomicAdd(h + A.np + c, A.dt * T(-0.5) * bz * bz * f * ab.vz()[c]);
+  }
+}
+
+// grho gathers h of the two velocity nodes each density value feeds
+template <typename T>
+__global__ void k_gather_rho(const T *h, double *grho, int nx, int nz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= nx || j >= nz) return;
+  const long long c = (long long)j * nx + i, np = (long long)nx * nz;
+  double s = (double)h[c] + (double)h[np + c];
+  if (i > 0) s += h[c - 1];
+  if (j > 0) s += h[np + c - nx];
+  grho[c] += s;
+}
+
+// sigma += -D^T dbar over every cell the velocity stencil reads (ghost rows
+// included; the images^T of the previous step folds them)
+template <typename T>
+__global__ void k_div_t(AdjArgs<T> A, Slot<T> ab, const T *dbar) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= A.nx || j >= A.nz) return;
+  const int nx = A.nx, nz = A.nz;
+  const long long c = (long long)j * nx + i, np = A.np;
+  ab.sxx()[c] -= tap_m_b(dbar, i, j, nx, nz, 0, A.Dx);
+  ab.sxz()[c] -= tap_p_b(dbar + np, i, j, nx, nz, 1, A.Dz) + tap_p_b(dbar + 2 * np, i, j, nx, nz, 0, A.Dx);
+  ab.szz()[c] -= tap_m_b(dbar + 3 * np, i, j, nx, nz, 1, A.Dz);
+}
+
+// FP64 misfit: 1/2 sum (d - obs)^2 (one block, deterministic order)
+template <typename T>
+__global__ void k_misfit(const T *tr, const T *obs, long long n, double *out) {
+  __shared__ double red[256];
+  double s = 0;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    const double d = (double)tr[k] - (double)obs[k];
+    s += d * d;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = 0.5 * red[0];
+}
+
+// ISO fold and the (vp, vs, rho, 1/Q) chain rule
+__global__ void k_velocity_grad(int kind, long long np, const double *g, const double *vp,
+                                const double *vs, const double *rho, const double *eps,
+                                const double *delta, double tau_scale, double *out) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= np) return;
+  const double grho = g[0 * np + c], g11 = g[1 * np + c], g13 = g[2 * np + c];
+  const double g33 = g[4 * np + c], g55 = g[6 * np + c], gtau = g[7 * np + c];
+  const double p = vp[c], s = vs[c], r = rho[c];
+  double gC33, gC55;
+  if (kind == VI_MEDIUM_ISO) {
+    // g13 slot carries dJ/dlambda, g55 slot dJ/dmu (already folded)
+    const double gl = g13, gm = g55;
+    gC33 = gl;          // lambda = rho (vp^2 - 2 vs^2): d/dvp via vp^2
+    gC55 = gm - 2 * gl; // mu = rho vs^2
+  } else {
+    const double e = eps ? eps[c] : 0.0, d = delta ? delta[c] : 0.0;
+    const double C33 = r * p * p, C55 = r * s * s;
+    const double A = C33 - C55, B = C33 * (1 + 2 * d) - C55;
+    const double sq = sqrt(fmax(A * B, 1e-300));
+    const double dC13_dC33 = (B + A * (1 + 2 * d)) / (2 * sq);
+    const double dC13_dC55 = (-B - A) / (2 * sq) - 1.0;
+    gC33 = g33 + g11 * (1 + 2 * e) + g13 * dC13_dC33;
+    gC55 = g55 + g13 * dC13_dC55;
+  }
+  out[0 * np + c] = gC33 * 2 * r * p;                 // dJ/dvp
+  out[1 * np + c] = gC55 * 2 * r * s;                 // dJ/dvs
+  out[2 * np + c] = grho + gC33 * p * p + gC55 * s * s;  // dJ/drho at fixed vp, vs
+  out[3 * np + c] = gtau * tau_scale;                 // dJ/d(1/Q)
+}
+
+__global__ void k_fold_iso(long long np, double *g) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= np) return;
+  // C11 = C33 = lambda + 2 mu, C13 = lambda, C55 = mu
+  const double g11 = g[1 * np + c], g13 = g[2 * np + c], g33 = g[4 * np + c], g55 = g[6 * np + c];
+  g[2 * np + c] = g11 + g13 + g33;
+  g[6 * np + c] = 2 * (g11 + g33) + g55;
+  g[1 * np + c] = 0;
+  g[4 * np + c] = 0;
+}
+
+}  // namespace
+
+template <typename T>
+static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, int nt, const T *obs,
+                         int K, int accumulate, double *grad, double *misfit, cudaStream_t st) {
+  const vi_config &c = p->cfg;
+  if (c.medium == VI_MEDIUM_TTI) return set_error(VI_ERR_ARG, "gradient: TTI media are not supported");
+  int rc = check_medium(p, m);
+  if (rc) return rc;
+  if (!shot || shot->nrec <= 0 || !obs) return set_error(VI_ERR_ARG, "gradient: needs receivers and observed traces");
+  if (!grad) return set_error(VI_ERR_ARG, "gradient: grad buffer is NULL");
+  if (nt <= 0) return set_error(VI_ERR_ARG, "gradient: nt must be positive");
+  if ((rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice"))) return rc;
+  if (K <= 0) K = (int)std::ceil(std::sqrt((double)nt));
+  if (K > nt) K = nt;
+  const int nck = (nt + K - 1) / K;
+  const long long np = (long long)c.nx * c.nz;
+  const int N = c.nsls;
+  const long long slot = Slot<T>::size(np, p->psix_plane, p->psiz_plane, N);
+  // workspace: checkpoints | segment (K + 1 slots) | adjoint slot | scratch (4 rbar/dbar, q, 2 h, 6 plain) | traces
+  const int nrec = shot->nrec;
+  const long long ntr = 2LL * nrec * nt;
+  const long long scratch = 4 * np + np + 2 * np + 6 * np;
+  const size_t need = sizeof(T) * ((size_t)(nck + K + 2) * slot + scratch + ntr) + 64;
+  size_t have = p->fwd_bytes;
+  if ((rc = ensure_buffer(p, &p->fwd, &have, need))) return rc;
+  p->fwd_bytes = have;
+  T *ck = (T *)p->fwd;
+  T *seg = ck + (size_t)nck * slot;
+  T *adj = seg + (size_t)(K + 1) * slot;
+  T *rbar = adj + slot;   // also dbar
+  T *q = rbar + 4 * np;
+  T *h = q + np;
+  T *pscr = h + 2 * np;   // plain-path scratch (6 planes)
+  T *tr = pscr + 6 * np;
+  auto mk = [&](T *b) { return Slot<T>{b, np, p->psix_plane, p->psiz_plane, N}; };
+  if ((rc = stage_shot<T>(p, shot, st))) return rc;
+  // plain forward step on a slot, in place (bind() points it at the slot)
+  vi_fields fdummy{};
+  fdummy.vx = fdummy.vz = fdummy.sxx = fdummy.szz = fdummy.sxz = (void *)ck;
+  fdummy.m = ck;
+  fdummy.m_plane_stride = np;
+  StepArgs<T> a = make_args<T>(p, m, &fdummy);
+  PlainExtras<T> x;
+  x.scratch = pscr;
+  x.fs = c.free_surface;
+  x.src = (const int4 *)p->dsrc;
+  x.amp = (const T *)p->damp;
+  x.nsrc = shot->nsrc;
+  x.wavelet = shot->nsrc ? (const T *)shot->wavelet_dev : nullptr;
+  x.wnt = shot->nsrc ? shot->wavelet_nt : 0;
+  x.rec = (const int2 *)p->drec;
+  x.nrec = nrec;
+  x.traces = nullptr;
+  x.tnt = nt;
+  auto bind = [&](StepArgs<T> &s, const Slot<T> &sl) {
+    s.vx = sl.vx(); s.vz = sl.vz(); s.sxx = sl.sxx(); s.szz = sl.szz(); s.sxz = sl.sxz();
+    s.m = sl.m(); s.mstride = np;
+    s.psix = s.psix_o = p->wx ? sl.psix() : nullptr;
+    s.psiz = s.psiz_o = p->hz ? sl.psiz() : nullptr;
+  };
+  const size_t sbytes = (size_t)slot * sizeof(T);
+  // plain-path scratch: cells outside the update region are read, never written
+  if ((rc = cuda_check(cudaMemsetAsync(pscr, 0, 6 * np * sizeof(T), st), "zero scratch"))) return rc;
+  // ---- forward sweep with checkpoints and traces ----
+  Slot<T> cur = mk(seg);
+  if ((rc = cuda_check(cudaMemsetAsync(seg, 0, sbytes, st), "zero state"))) return rc;
+  bind(a, cur);
+  x.traces = tr;
+  for (int it = 0; it < nt; ++it) {
+    if (it % K == 0)
+      if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, seg, sbytes, cudaMemcpyDeviceToDevice, st),
+                           "checkpoint")))
+        return rc;
+    plain_step<T>(a, x, c.medium, it, st);
+  }
+  x.traces = nullptr;
+  if (shot->traces_dev && shot->traces_nt >= nt) {
+    for (int k = 0; k < 2 * nrec; ++k)
+      cudaMemcpyAsync((T *)shot->traces_dev + (size_t)k * shot->traces_nt, tr + (size_t)k * nt,
+                      nt * sizeof(T), cudaMemcpyDeviceToDevice, st);
+  }
+  double *dmis = (double *)(tr + ntr);
+  dmis = (double *)(((uintptr_t)dmis + 15) / 16 * 16);
+  k_misfit<T><<<1, 256, 0, st>>>(tr, obs, ntr, dmis);
+  // ---- adjoint sweep ----
+  AdjArgs<T> A;
+  A.nx = c.nx; A.nz = c.nz; A.nsls = N; A.kind = c.medium; A.fs = c.free_surface;
+  A.Lx = p->Lx; A.Rx = p->Rx; A.Tz = p->Tz; A.Bz = p->Bz; A.wx = p->wx; A.hz = p->hz;
+  A.dt = (T)c.dt;
+  for (int k = 0; k < 4; ++k) {
+    A.Dx[k] = (T)(kD8[k] / c.dx);
+    A.Dz[k] = (T)(kD8[k] / c.dz);
+  }
+  for (int n = 0; n < N; ++n) {  // the forward step's memory-variable coefficients
+    A.a1[n] = a.a1[n];
+    A.a2[n] = a.a2[n];
+  }
+  A.rho = (const T *)m->rho; A.c11 = (const T *)m->c11; A.c13 = (const T *)m->c13;
+  A.c33 = (const T *)m->c33; A.c55 = (const T *)m->c55; A.tau = (const T *)m->tau;
+  A.tx = (const T *)p->tabx; A.tz = (const T *)p->tabz;
+  A.np = np; A.psix_plane = p->psix_plane; A.psiz_plane = p->psiz_plane;
+  Slot<T> ab = mk(adj);
+  if ((rc = cuda_check(cudaMemsetAsync(adj, 0, sbytes, st), "zero adjoint"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(rbar, 0, 7 * np * sizeof(T), st), "zero scratch"))) return rc;
+  if (!accumulate)
+    if ((rc = cuda_check(cudaMemsetAsync(grad, 0, 8 * np * sizeof(double), st), "zero gradient"))) return rc;
+  double *gr = grad, *g11 = grad + np, *g13 = grad + 2 * np, *g33 = grad + 4 * np;
+  double *g55 = grad + 6 * np, *gt = grad + 7 * np;
+  const dim3 blk(32, 8);
+  const dim3 gU((c.nx - 2 * L + 31) / 32, (c.nz - 2 * L + 7) / 8);
+  const dim3 gA((c.nx + 31) / 32, (c.nz + 7) / 8);
+  for (int qseg = nck - 1; qseg >= 0; --qseg) {
+    const int s0 = qseg * K, s1 = std::min(nt, s0 + K);
+    // recompute the segment: seg[k] = state before step s0 + k
+    if ((rc = cuda_check(cudaMemcpyAsync(seg, ck + (size_t)qseg * slot, sbytes, cudaMemcpyDeviceToDevice, st),
+                         "restore checkpoint")))
+      return rc;
+    for (int k = 0; k < s1 - s0; ++k) {
+      T *nxt = seg + (size_t)(k + 1) * slot;
+      if ((rc = cuda_check(cudaMemcpyAsync(nxt, seg + (size_t)k * slot, sbytes, cudaMemcpyDeviceToDevice, st),
+                           "segment copy")))
+        return rc;
+      bind(a, mk(nxt));
+      plain_step<T>(a, x, c.medium, s0 + k, st);
+    }
+    for (int it = s1 - 1; it >= s0; --it) {
+      const Slot<T> x0 = mk(seg + (size_t)(it - s0) * slot), x1 = mk(seg + (size_t)(it - s0 + 1) * slot);
+      if (c.free_surface) k_mirror_t<T><<<(c.nx + 127) / 128, 128, 0, st>>>(ab.szz(), ab.sxz(), c.nx);
+      k_stress_t<T><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt);
+      k_gather_c55<T><<<gA, blk, 0, st>>>(q, g55, c.nx, c.nz);
+      k_rates_t<T><<<gU, blk, 0, st>>>(A, ab, rbar);
+      k_residual<T><<<(nrec + 127) / 128, 128, 0, st>>>(ab, x1, (const int2 *)p->drec, nrec, obs, nt, it, c.nx);
+      k_vel_t<T><<<gU, blk, 0, st>>>(A, x0, ab, rbar, h);
+      if (shot->nsrc > 0)
+        k_force_rho_t<T><<<(shot->nsrc + 127) / 128, 128, 0, st>>>(A, ab, (const int4 *)p->dsrc,
+                                                                     (const T *)p->damp, shot->nsrc,
+                                                                     (const T *)shot->wavelet_dev,
+                                                                     shot->wavelet_nt, it, h);
+      k_gather_rho<T><<<gA, blk, 0, st>>>(h, gr, c.nx, c.nz);
+      k_div_t<T><<<gA, blk, 0, st>>>(A, ab, rbar);
+    }
+  }
+  if (c.medium == VI_MEDIUM_ISO) k_fold_iso<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(np, grad);
+  p->last_kernel = 1;
+  if ((rc = cuda_check(cudaGetLastError(), "gradient launch"))) return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(misfit, dmis, sizeof(double), cudaMemcpyDeviceToHost, st), "misfit")))
+    return rc;
+  return cuda_check(cudaStreamSynchronize(st), "gradient");
+}
+
+}  // namespace vb
+
+using namespace vb;
+
+extern "C" int vi_gradient(vi_plan *p, const vi_medium *med_dev, const vi_shot *shot, int32_t nt,
+                           const void *obs_dev, int32_t checkpoint_every, int32_t accumulate,
+                           double *grad_dev, double *misfit_host, void *stream) {
+  if (!p || !misfit_host) return set_error(VI_ERR_ARG, "gradient: NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  return p->cfg.precision == VI_F64
+             ? gradient_impl<double>(p, med_dev, shot, nt, (const double *)obs_dev, checkpoint_every,
+                                     accumulate, grad_dev, misfit_host, st)
+             : gradient_impl<float>(p, med_dev, shot, nt, (const float *)obs_dev, checkpoint_every,
+                                    accumulate, grad_dev, misfit_host, st);
+}
+
+extern "C" int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const double *vp,
+                                    const double *vs, const double *rho, const double *eps,
+                                    const double *delta, double tau_scale, double *out4, void *stream) {
+  if (!grad8 || !vp || !vs || !rho || !out4 || np <= 0)
+    return set_error(VI_ERR_ARG, "gradient_velocity: NULL argument");
+  if (medium != VI_MEDIUM_ISO && medium != VI_MEDIUM_VTI)
+    return set_error(VI_ERR_ARG, "gradient_velocity: ISO or VTI only");
+  k_velocity_grad<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      medium, np, grad8, vp, vs, rho, eps, delta, tau_scale, out4);
+  return cuda_check(cudaGetLastError(), "gradient_velocity launch");
+}

@@ -1,0 +1,432 @@
+// batch.cu — many shots of different grids and step counts advancing
+// together: one kernel launch per time step covers the tiles of every shot
+// still running, and the whole sequence of launches is one CUDA graph.
+//
+// Each shot keeps its own plan (CPML tables and ψ, the second state copy,
+// source/receiver lists); the batch adds device arrays of per-shot step
+// arguments, extras and tensor maps (both ping-pong parities) that the
+// batched TMA kernel indexes per tile.  Shots are processed in descending
+// step-count order so the shots active at step it are a prefix of the
+// order and a launch covers items [0, prefix[active]).
+//
+// The autotuner picks the kernel form (two-stage persistent tiles or
+// one-stage tiles) by timing a few steps of each on the bound shots and
+// caches the choice per (medium, precision, mechanisms, grid set).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "fused_tma.cuh"
+#include "plan.cuh"
+
+struct vi_batch {
+  int n = 0;
+  int kind = 0, precision = 0, nsls = 0, device = 0, nsm = 148;
+  std::vector<vi_plan *> plans;
+  std::vector<vi_medium> med;
+  std::vector<vi_fields> fields;
+  std::vector<int> nt;
+  std::vector<std::vector<vi_source>> src;
+  std::vector<std::vector<vi_receiver>> rec;
+  std::vector<vi_shot> shot;
+  std::vector<char> bound;
+  // device arrays
+  void *dev = nullptr;
+  size_t dev_bytes = 0;
+  int *err = nullptr;
+  // cached graph of the whole run (valid while nothing is re-bound)
+  cudaGraphExec_t graph = nullptr;
+  bool graph_persist = true;
+  bool dirty = true;
+  int persist = -1;  // kernel form: -1 untuned, 0 one-stage, 1 two-stage persistent
+  std::vector<int> order;
+  std::vector<int> prefix;
+  int max_nt = 0;
+};
+
+namespace vb {
+
+static std::map<std::string, int> g_tuned;  // kernel form chosen per problem class
+
+static std::string tune_key(const vi_batch *b) {
+  std::vector<std::pair<int, int>> g;
+  for (int i = 0; i < b->n; ++i) g.emplace_back(b->plans[i]->cfg.nx, b->plans[i]->cfg.nz);
+  std::sort(g.begin(), g.end());
+  g.erase(std::unique(g.begin(), g.end()), g.end());
+  std::string k = std::to_string(b->kind) + "/" + std::to_string(b->precision) + "/" +
+                  std::to_string(b->nsls);
+  for (auto &p : g) k += "/" + std::to_string(p.first) + "x" + std::to_string(p.second);
+  return k;
+}
+
+// Builds every per-shot device structure for one kernel form and uploads it.
+template <typename T>
+static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) {
+  const TmaBoxes bx = tma_boxes(b->kind, b->nsls, (int)sizeof(T), persist);
+  if (!bx.ok) return set_error(VI_ERR_ARG, "batch: the TMA-staged step does not fit this medium");
+  const int n = b->n;
+  std::vector<StepArgs<T>> args(2 * n);
+  std::vector<FusedExtras<T>> ext(n);
+  std::vector<TmaMaps> maps(2 * n);
+  std::vector<int> ntiles(n);
+  int rc;
+  for (int i = 0; i < n; ++i) {
+    vi_plan *p = b->plans[i];
+    const vi_config &c = p->cfg;
+    const size_t np = (size_t)c.nx * c.nz;
+    const int nstate = 5 + 3 * c.nsls;
+    if (!p->alt) {
+      size_t have = 0;
+      if ((rc = ensure_buffer(p, &p->alt, &have, nstate * np * sizeof(T)))) return rc;
+      if ((rc = cuda_check(cudaMemsetAsync(p->alt, 0, nstate * np * sizeof(T), st), "zero alt state")))
+        return rc;
+    }
+    if ((rc = stage_shot<T>(p, &b->shot[i], st))) return rc;
+    int ntx, ntz;
+    std::vector<int> off;
+    std::vector<int4> ent;
+    build_tile_lists(c.nx, c.nz, bx.TX, bx.TZ, bx.HV, &b->shot[i], off, ent, ntx, ntz);
+    int *d_off = nullptr;
+    int4 *d_ent = nullptr;
+    if ((rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent))) return rc;
+    ntiles[i] = ntx * ntz;
+    StepArgs<T> a = make_args<T>(p, &b->med[i], &b->fields[i]);
+    T *user[5] = {a.vx, a.vz, a.sxx, a.szz, a.sxz};
+    T *alt = (T *)p->alt;
+    T *alt_st[5];
+    for (int q = 0; q < 5; ++q) alt_st[q] = alt + q * np;
+    T *psix0 = (T *)p->psix, *psiz0 = (T *)p->psiz;
+    p->psi_cur = 0;  // a batch run starts from rest: psi is reset below
+    for (int par = 0; par < 2; ++par) {
+      StepArgs<T> s = a;
+      T *const *in = par == 0 ? user : alt_st;
+      T *const *out = par == 0 ? alt_st : user;
+      s.vx = in[0]; s.vz = in[1]; s.sxx = in[2]; s.szz = in[3]; s.sxz = in[4];
+      s.vx_o = out[0]; s.vz_o = out[1]; s.sxx_o = out[2]; s.szz_o = out[3]; s.sxz_o = out[4];
+      s.m = par == 0 ? a.m : alt + 5 * np;
+      s.mstride = par == 0 ? a.mstride : (long long)np;
+      s.m_o = par == 0 ? alt + 5 * np : a.m;
+      s.mstride_o = par == 0 ? (long long)np : a.mstride;
+      s.psix = psix0 ? psix0 + par * kPsiPerSet * p->psix_plane : nullptr;
+      s.psix_o = psix0 ? psix0 + (1 - par) * kPsiPerSet * p->psix_plane : nullptr;
+      s.psiz = psiz0 ? psiz0 + par * kPsiPerSet * p->psiz_plane : nullptr;
+      s.psiz_o = psiz0 ? psiz0 + (1 - par) * kPsiPerSet * p->psiz_plane : nullptr;
+      args[2 * i + par] = s;
+      if ((rc = encode_parity<T>(maps[2 * i + par], bx, c, in, s.m, s.mstride, s))) return rc;
+    }
+    FusedExtras<T> &x = ext[i];
+    x.ntx = ntx;
+    x.fs = c.free_surface;
+    x.it = 0;
+    x.tile_off = d_off;
+    x.tile_ent = d_ent;
+    x.amp = (const T *)p->damp;
+    const vi_shot &sh = b->shot[i];
+    x.wavelet = sh.nsrc ? (const T *)sh.wavelet_dev : nullptr;
+    x.wnt = sh.nsrc ? sh.wavelet_nt : 0;
+    x.traces = sh.nrec ? (T *)sh.traces_dev : nullptr;
+    x.tnt = sh.nrec ? sh.traces_nt : 0;
+    x.nrec = sh.nrec;
+    x.err = b->err;
+  }
+  // descending step count: the shots active at step it form a prefix
+  b->order.resize(n);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  std::stable_sort(b->order.begin(), b->order.end(),
+                   [&](int x, int y) { return b->nt[x] > b->nt[y]; });
+  b->prefix.assign(n + 1, 0);
+  for (int q = 0; q < n; ++q) b->prefix[q + 1] = b->prefix[q] + ntiles[b->order[q]];
+  b->max_nt = n ? b->nt[b->order[0]] : 0;
+  // one device block: args | ext | maps | prefix | order
+  auto up = [](size_t x) { return (x + 127) / 128 * 128; };
+  const size_t o_args = 0, o_ext = up(o_args + args.size() * sizeof(StepArgs<T>));
+  const size_t o_maps = up(o_ext + ext.size() * sizeof(FusedExtras<T>));
+  const size_t o_pre = up(o_maps + maps.size() * sizeof(TmaMaps));
+  const size_t o_ord = up(o_pre + b->prefix.size() * sizeof(int));
+  const size_t total = up(o_ord + b->order.size() * sizeof(int));
+  if (b->dev_bytes < total) {
+    if (b->dev) cudaFree(b->dev);
+    b->dev = nullptr;
+    b->dev_bytes = 0;
+    if (cudaMalloc(&b->dev, total) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(VI_ERR_BUDGET, "batch: cudaMalloc of the shot table failed");
+    }
+    b->dev_bytes = total;
+  }
+  std::vector<char> host(total, 0);
+  std::memcpy(host.data() + o_args, args.data(), args.size() * sizeof(StepArgs<T>));
+  std::memcpy(host.data() + o_ext, ext.data(), ext.size() * sizeof(FusedExtras<T>));
+  std::memcpy(host.data() + o_maps, maps.data(), maps.size() * sizeof(TmaMaps));
+  std::memcpy(host.data() + o_pre, b->prefix.data(), b->prefix.size() * sizeof(int));
+  std::memcpy(host.data() + o_ord, b->order.data(), b->order.size() * sizeof(int));
+  if ((rc = cuda_check(cudaMemcpyAsync(b->dev, host.data(), total, cudaMemcpyHostToDevice, st),
+                       "upload batch table")))
+    return rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(st), "upload batch table"))) return rc;
+  char *d = (char *)b->dev;
+  bd.args = (const StepArgs<T> *)(d + o_args);
+  bd.ext = (const FusedExtras<T> *)(d + o_ext);
+  bd.maps = (const TmaMaps *)(d + o_maps);
+  bd.prefix = (const int *)(d + o_pre);
+  bd.order = (const int *)(d + o_ord);
+  bd.nshots = n;
+  bd.err = b->err;
+  return VI_OK;
+}
+
+// Items (tiles of active shots) at step it.
+static int items_at(const vi_batch *b, int it) {
+  int a = 0;
+  while (a < b->n && b->nt[b->order[a]] > it) ++a;
+  return b->prefix[a];
+}
+
+template <typename T>
+static int launch_steps(vi_batch *b, const BatchDev<T> &bd, bool persist, int it0, int it1,
+                        cudaStream_t st) {
+  for (int it = it0; it < it1; ++it) {
+    const int nitems = items_at(b, it);
+    if (nitems == 0) break;
+    int rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, it, nitems, b->nsm, persist, st);
+    if (rc) return rc;
+  }
+  return cuda_check(cudaGetLastError(), "batch launch");
+}
+
+// Zeroes every shot's fields and psi (the state a forward solve starts from).
+template <typename T>
+static int reset_state(vi_batch *b, cudaStream_t st) {
+  int rc;
+  for (int i = 0; i < b->n; ++i) {
+    vi_plan *p = b->plans[i];
+    const size_t pb = (size_t)p->cfg.nx * p->cfg.nz * sizeof(T);
+    const vi_fields &f = b->fields[i];
+    void *planes[5] = {f.vx, f.vz, f.sxx, f.szz, f.sxz};
+    for (void *q : planes)
+      if ((rc = cuda_check(cudaMemsetAsync(q, 0, pb, st), "reset fields"))) return rc;
+    for (int q = 0; q < 3 * p->cfg.nsls; ++q)
+      if ((rc = cuda_check(cudaMemsetAsync((char *)f.m + q * f.m_plane_stride * sizeof(T), 0, pb, st),
+                           "reset memory variables")))
+        return rc;
+    if ((rc = vi_plan_reset(p, st))) return rc;
+  }
+  return VI_OK;
+}
+
+template <typename T>
+static int tune(vi_batch *b, cudaStream_t st) {
+  const std::string key = tune_key(b);
+  auto hit = g_tuned.find(key);
+  if (hit != g_tuned.end()) {
+    b->persist = hit->second;
+    return VI_OK;
+  }
+  float best = 1e30f;
+  int choice = 1;
+  const int forms = sizeof(T) == 4 ? 2 : 1;  // double precision has one form
+  for (int f = 0; f < forms; ++f) {
+    const bool persist = f == 0;
+    BatchDev<T> bd;
+    int rc = prepare<T>(b, persist, st, bd);
+    if (rc == VI_ERR_ARG) continue;
+    if (rc) return rc;
+    const int steps = std::min(8, b->max_nt);
+    if ((rc = launch_steps<T>(b, bd, persist, 0, 2, st))) return rc;  // warm-up
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    rc = launch_steps<T>(b, bd, persist, 0, steps, st);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (ms < best) {
+      best = ms;
+      choice = persist ? 1 : 0;
+    }
+  }
+  b->persist = choice;
+  g_tuned[key] = choice;
+  // tuning advanced the shots: put them back at rest
+  return reset_state<T>(b, st);
+}
+
+template <typename T>
+static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
+  for (int i = 0; i < b->n; ++i)
+    if (!b->bound[i]) return set_error(VI_ERR_STATE, "batch: shot " + std::to_string(i) + " is not bound");
+  int rc = cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+  if (rc) return rc;
+  const bool use_graph = (flags & VI_BATCH_NO_GRAPH) == 0;
+  if (b->persist < 0 || (flags & VI_BATCH_RETUNE)) {
+    if (flags & VI_BATCH_RETUNE) g_tuned.erase(tune_key(b));
+    if ((rc = tune<T>(b, st))) return rc;
+    b->dirty = true;
+  }
+  const bool persist = b->persist == 1;
+  for (int i = 0; i < b->n; ++i)
+    if ((rc = vi_plan_reset(b->plans[i], st))) return rc;
+  if (b->dirty || !use_graph || b->graph_persist != persist) {
+    BatchDev<T> bd;
+    if ((rc = prepare<T>(b, persist, st, bd))) return rc;
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    if (use_graph) {
+      // kernel attributes are set outside the capture
+      if ((rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, 0, 0, b->nsm, persist, st))) return rc;
+      cudaStream_t cs;
+      if ((rc = cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream")))
+        return rc;
+      cudaGraph_t g = nullptr;
+      rc = cuda_check(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+      if (!rc) {
+        const int lrc = launch_steps<T>(b, bd, persist, 0, b->max_nt, cs);
+        rc = cuda_check(cudaStreamEndCapture(cs, &g), "end capture");
+        if (!rc) rc = lrc;
+      }
+      if (!rc) rc = cuda_check(cudaGraphInstantiate(&b->graph, g, 0), "instantiate graph");
+      if (g) cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      if (rc) return rc;
+      b->graph_persist = persist;
+      b->dirty = false;
+    } else {
+      if ((rc = launch_steps<T>(b, bd, persist, 0, b->max_nt, st))) return rc;
+    }
+  }
+  if (use_graph && (rc = cuda_check(cudaGraphLaunch(b->graph, st), "graph launch"))) return rc;
+  // shots with an odd step count end in the plan's copy: bring them back
+  for (int i = 0; i < b->n; ++i) {
+    if (b->nt[i] % 2 == 0) continue;
+    vi_plan *p = b->plans[i];
+    const size_t np = (size_t)p->cfg.nx * p->cfg.nz;
+    T *alt = (T *)p->alt;
+    const vi_fields &f = b->fields[i];
+    void *user[5] = {f.vx, f.vz, f.sxx, f.szz, f.sxz};
+    for (int q = 0; q < 5; ++q)
+      if ((rc = cuda_check(cudaMemcpyAsync(user[q], alt + q * np, np * sizeof(T), cudaMemcpyDeviceToDevice, st),
+                           "copy back fields")))
+        return rc;
+    for (int q = 0; q < 3 * p->cfg.nsls; ++q)
+      if ((rc = cuda_check(cudaMemcpyAsync((T *)f.m + q * f.m_plane_stride, alt + (5 + q) * np,
+                                           np * sizeof(T), cudaMemcpyDeviceToDevice, st),
+                           "copy back memory variables")))
+        return rc;
+  }
+  return cuda_check(cudaGetLastError(), "batch run");
+}
+
+}  // namespace vb
+
+using namespace vb;
+
+extern "C" int vi_batch_create(const vi_config *cfgs, int32_t nshots, vi_batch **out) {
+  if (!out || !cfgs || nshots <= 0) return set_error(VI_ERR_ARG, "batch: bad arguments");
+  *out = nullptr;
+  for (int i = 1; i < nshots; ++i)
+    if (cfgs[i].medium != cfgs[0].medium || cfgs[i].precision != cfgs[0].precision ||
+        cfgs[i].nsls != cfgs[0].nsls)
+      return set_error(VI_ERR_ARG, "batch: shots must share medium kind, precision and nsls");
+  vi_batch *b = new vi_batch();
+  b->n = nshots;
+  b->kind = cfgs[0].medium;
+  b->precision = cfgs[0].precision;
+  b->nsls = cfgs[0].nsls;
+  cudaGetDevice(&b->device);
+  if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess)
+    b->nsm = 148;
+  for (int i = 0; i < nshots; ++i)
+    if ((cfgs[i].nx % 4) != 0) {
+      delete b;
+      return set_error(VI_ERR_ARG, "batch: every shot needs nx % 4 == 0 (TMA-staged tiles)");
+    }
+  b->plans.assign(nshots, nullptr);
+  for (int i = 0; i < nshots; ++i) {
+    int rc = vi_plan_create(&cfgs[i], &b->plans[i]);
+    if (rc) {
+      vi_batch_destroy(b);
+      return rc;
+    }
+  }
+  b->med.assign(nshots, vi_medium{});
+  b->fields.assign(nshots, vi_fields{});
+  b->nt.assign(nshots, 0);
+  b->src.resize(nshots);
+  b->rec.resize(nshots);
+  b->shot.assign(nshots, vi_shot{});
+  b->bound.assign(nshots, 0);
+  if (cudaMalloc(&b->err, 16) != cudaSuccess || cudaMemset(b->err, 0, 16) != cudaSuccess) {
+    cudaGetLastError();
+    vi_batch_destroy(b);
+    return set_error(VI_ERR_BUDGET, "batch: error word allocation failed");
+  }
+  *out = b;
+  return VI_OK;
+}
+
+extern "C" int vi_batch_destroy(vi_batch *b) {
+  if (!b) return VI_OK;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->dev) cudaFree(b->dev);
+  if (b->err) cudaFree(b->err);
+  for (vi_plan *p : b->plans) vi_plan_destroy(p);
+  delete b;
+  return VI_OK;
+}
+
+extern "C" int vi_batch_set_shot(vi_batch *b, int32_t i, const vi_medium *med_dev,
+                                 const vi_fields *fields_dev, const vi_shot *shot, int32_t nt) {
+  if (!b || i < 0 || i >= b->n) return set_error(VI_ERR_ARG, "batch: bad shot index");
+  if (nt < 0) return set_error(VI_ERR_ARG, "batch: negative step count");
+  vi_plan *p = b->plans[i];
+  int rc = check_medium(p, med_dev);
+  if (rc) return rc;
+  rc = check_fields(p, fields_dev);
+  if (rc) return rc;
+  b->med[i] = *med_dev;
+  b->fields[i] = *fields_dev;
+  b->nt[i] = nt;
+  vi_shot s{};
+  if (shot) {
+    s = *shot;
+    b->src[i].assign(shot->src_host, shot->src_host + (shot->nsrc > 0 ? shot->nsrc : 0));
+    b->rec[i].assign(shot->rec_host, shot->rec_host + (shot->nrec > 0 ? shot->nrec : 0));
+    s.src_host = b->src[i].data();
+    s.rec_host = b->rec[i].data();
+  }
+  b->shot[i] = s;
+  b->bound[i] = 1;
+  b->dirty = true;
+  return VI_OK;
+}
+
+extern "C" int vi_batch_run(vi_batch *b, int32_t flags, void *stream) {
+  if (!b) return set_error(VI_ERR_ARG, "batch is NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  return b->precision == VI_F64 ? run_impl<double>(b, flags, st) : run_impl<float>(b, flags, st);
+}
+
+extern "C" int vi_batch_status(vi_batch *b, void *stream, int32_t *kernel_form) {
+  if (!b) return set_error(VI_ERR_ARG, "batch is NULL");
+  int rc = cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "batch status");
+  if (rc) return rc;
+  if (kernel_form) *kernel_form = b->persist;
+  int flag = 0;
+  rc = cuda_check(cudaMemcpy(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
+  if (rc) return rc;
+  if (flag) {
+    cudaMemset(b->err, 0, sizeof(int));
+    return set_error(VI_ERR_TIMEOUT, "batch: a bounded device wait gave up");
+  }
+  return VI_OK;
+}

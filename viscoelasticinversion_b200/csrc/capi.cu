@@ -134,7 +134,7 @@ static int upload_tables(vi_plan *p) {
 }
 
 template <typename T>
-static StepArgs<T> make_args(const vi_plan *p, const vi_medium *m, const vi_fields *f) {
+StepArgs<T> make_args(const vi_plan *p, const vi_medium *m, const vi_fields *f) {
   const vi_config &c = p->cfg;
   StepArgs<T> a;
   std::memset(&a, 0, sizeof(a));
@@ -180,7 +180,7 @@ static StepArgs<T> make_args(const vi_plan *p, const vi_medium *m, const vi_fiel
   return a;
 }
 
-static int check_medium(const vi_plan *p, const vi_medium *m) {
+int check_medium(const vi_plan *p, const vi_medium *m) {
   if (!m) return set_error(VI_ERR_ARG, "medium is NULL");
   const int k = p->cfg.medium;
   if (!m->rho || !m->c13 || !m->c55) return set_error(VI_ERR_ARG, "medium: rho, c13, c55 required");
@@ -192,7 +192,7 @@ static int check_medium(const vi_plan *p, const vi_medium *m) {
   return VI_OK;
 }
 
-static int check_fields(const vi_plan *p, const vi_fields *f) {
+int check_fields(const vi_plan *p, const vi_fields *f) {
   if (!f) return set_error(VI_ERR_ARG, "fields is NULL");
   if (!f->vx || !f->vz || !f->sxx || !f->szz || !f->sxz)
     return set_error(VI_ERR_ARG, "fields: vx, vz, sxx, szz, sxz required");
@@ -210,7 +210,7 @@ static bool in_update_region(const vi_config &c, int i, int j) {
 
 // Copies the shot's source / receiver lists to the plan's device buffers.
 template <typename T>
-static int stage_shot(vi_plan *p, const vi_shot *s, cudaStream_t st) {
+int stage_shot(vi_plan *p, const vi_shot *s, cudaStream_t st) {
   if (!s) return VI_OK;
   if (s->nsrc < 0 || s->nrec < 0) return set_error(VI_ERR_ARG, "negative source/receiver count");
   if (s->nsrc > 0) {
@@ -333,6 +333,11 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   if (variant == 1) p->last_kernel = 1;
   return cuda_check(cudaGetLastError(), "step launch");
 }
+
+template StepArgs<float> make_args<float>(const vi_plan *, const vi_medium *, const vi_fields *);
+template StepArgs<double> make_args<double>(const vi_plan *, const vi_medium *, const vi_fields *);
+template int stage_shot<float>(vi_plan *, const vi_shot *, cudaStream_t);
+template int stage_shot<double>(vi_plan *, const vi_shot *, cudaStream_t);
 
 }  // namespace vb
 

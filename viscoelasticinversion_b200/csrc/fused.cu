@@ -434,7 +434,7 @@ static bool aligned16(const void *ptr) { return ((uintptr_t)ptr & 15) == 0; }
 // Tensor maps of one ping-pong parity: the input state (sigma, v, M) and the
 // medium.
 template <typename T>
-static int encode_parity(TmaMaps &m, const TmaBoxes &b, const vi_config &c, T *const in[5],
+int encode_parity(TmaMaps &m, const TmaBoxes &b, const vi_config &c, T *const in[5],
                          const T *min, long long mstride, const StepArgs<T> &a) {
   const int e = sizeof(T), nx = c.nx, nz = c.nz;
   int rc;
@@ -595,6 +595,10 @@ int fused_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   return VI_OK;
 }
 
+template int encode_parity<float>(TmaMaps &, const TmaBoxes &, const vi_config &, float *const[5],
+                                  const float *, long long, const StepArgs<float> &);
+template int encode_parity<double>(TmaMaps &, const TmaBoxes &, const vi_config &, double *const[5],
+                                   const double *, long long, const StepArgs<double> &);
 template int fused_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t, int);
 template int fused_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int, cudaStream_t, int);
 

@@ -674,6 +674,130 @@ __global__ void __launch_bounds__(TmaPick<T, KIND, NSLS, PERSIST>::Lay::NT)
   }
 }
 
+// Many shots advancing one time step together: the launch covers the tiles
+// of every active shot (shots sorted by step count, so the active ones are
+// a prefix), each item reads its shot's arguments and tensor maps from
+// device memory.  Same staging, pipeline and arithmetic as k_fused_tma.
+template <typename T, int KIND, int NSLS, bool PERSIST>
+__global__ void __launch_bounds__(TmaPick<T, KIND, NSLS, PERSIST>::Lay::NT)
+    k_fused_tma_batch(const BatchDev<T> b, int it, int nitems) {
+  using G = typename TmaPick<T, KIND, NSLS, PERSIST>::Lay;
+  constexpr int ST = G::STAGES;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  T *stage0 = sm + G::O_STAGE;
+  T *s_e = sm + G::O_E;
+  const int tid = threadIdx.x;
+  const int G0 = gridDim.x;
+  const int par = it & 1;
+  auto locate = [&](int item, int &shot, int &tile) {
+    int lo = 0, hi = b.nshots - 1;  // largest p with prefix[p] <= item
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (b.prefix[mid] <= item)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    shot = b.order[lo];
+    tile = item - b.prefix[lo];
+  };
+  auto issue_item = [&](int s, int item) {
+    int shot, tile;
+    locate(item, shot, tile);
+    const int ntx = b.ext[shot].ntx;
+    const int x0 = L + (tile % ntx) * G::TX, z0 = L + (tile / ntx) * G::TZ;
+    issue_tile<G, T>(stage0 + s * G::STAGE, &bars[s], b.maps[2 * shot + par], x0, z0);
+  };
+  if (tid == 0)
+    for (int s = 0; s < ST; ++s) mbar_init(&bars[s], 1);
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < ST; ++s)
+      if (blockIdx.x + s * G0 < nitems) issue_item(s, blockIdx.x + s * G0);
+  int j = 0;
+  for (int item = blockIdx.x; item < nitems; item += G0, ++j) {
+    const int s = ST == 2 ? (j & 1) : 0;
+    const uint32_t parity = ST == 2 ? ((j >> 1) & 1) : (j & 1);
+    int shot, tile;
+    locate(item, shot, tile);
+    FusedExtras<T> x = b.ext[shot];
+    x.it = it;
+    const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
+    const bool ok = mbar_wait_bounded(&bars[s], parity, 1u << 22);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(b.err, 1);
+        mbar_wait_bounded(&bars[s], parity, 1u << 22);
+        if (ST == 2 && item + G0 < nitems) mbar_wait_bounded(&bars[s ^ 1], ((j + 1) >> 1) & 1, 1u << 22);
+      }
+      return;
+    }
+    compute_tile<G, T, KIND, NSLS>(b.args[2 * shot + par], x, stage0 + s * G::STAGE, s_e, tile, e0, e1);
+    __syncthreads();
+    if (tid == 0) {
+      const int nxt = item + ST * G0;
+      if (nxt < nitems) {
+        fence_proxy_async_smem();
+        issue_item(s, nxt);
+      }
+    }
+  }
+}
+
+template <typename T, int KIND, int NSLS, bool PERSIST>
+static int launch_batch_one(const BatchDev<T> &b, int it, int nitems, int nsm, cudaStream_t st) {
+  if constexpr (!TmaPick<T, KIND, NSLS, PERSIST>::OK) {
+    return set_error(VI_ERR_ARG, "TMA-staged step does not fit shared memory for this medium");
+  } else {
+    using G = typename TmaPick<T, KIND, NSLS, PERSIST>::Lay;
+    static unsigned long long attr_set = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(attr_set & (1ULL << dev))) {
+      cudaError_t e = cudaFuncSetAttribute(k_fused_tma_batch<T, KIND, NSLS, PERSIST>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, G::BYTES);
+      if (e != cudaSuccess) return cuda_check(e, "batch step smem attribute");
+      attr_set |= 1ULL << dev;
+    }
+    int per = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_tma_batch<T, KIND, NSLS, PERSIST>,
+                                                      G::NT, G::BYTES) != cudaSuccess || per < 1) {
+      cudaGetLastError();
+      per = 1;
+    }
+    if (nitems <= 0) return VI_OK;  // attribute set-up only
+    const int cap = G::STAGES == 2 ? per * nsm : nitems;
+    const int grid = nitems < cap ? nitems : cap;
+    k_fused_tma_batch<T, KIND, NSLS, PERSIST><<<grid, G::NT, G::BYTES, st>>>(b, it, nitems);
+    return VI_OK;
+  }
+}
+
+template <typename T>
+int launch_fused_tma_batch(int kind, int nsls, const BatchDev<T> &b, int it, int nitems, int nsm,
+                           bool persist, cudaStream_t st) {
+  constexpr bool kSplit = sizeof(T) == 4;
+#define VB_CASE(K, N)                                                                        \
+  if (kind == K && nsls == N) {                                                              \
+    if (kSplit && !persist) return launch_batch_one<T, K, N, !kSplit>(b, it, nitems, nsm, st); \
+    return launch_batch_one<T, K, N, true>(b, it, nitems, nsm, st);                          \
+  }
+#define VB_KIND(K) VB_CASE(K, 0) VB_CASE(K, 1) VB_CASE(K, 2) VB_CASE(K, 3) VB_CASE(K, 4) VB_CASE(K, 5)
+  VB_KIND(VI_MEDIUM_ISO)
+  VB_KIND(VI_MEDIUM_VTI)
+  VB_KIND(VI_MEDIUM_TTI)
+#undef VB_KIND
+#undef VB_CASE
+  return set_error(VI_ERR_ARG, "unsupported medium / nsls combination");
+}
+
+template int launch_fused_tma_batch<float>(int, int, const BatchDev<float> &, int, int, int, bool,
+                                           cudaStream_t);
+template int launch_fused_tma_batch<double>(int, int, const BatchDev<double> &, int, int, int, bool,
+                                            cudaStream_t);
+
 template <typename T, int KIND, int NSLS, bool PERSIST>
 static int launch_tma_one(const StepArgs<T> &a, const FusedExtras<T> &x, const TmaMaps &maps,
                           int ntiles, int nsm, cudaStream_t st) {

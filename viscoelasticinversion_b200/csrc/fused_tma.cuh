@@ -101,6 +101,28 @@ template <typename T>
 int launch_fused_tma(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
                      const TmaMaps &maps, int ntiles, int nsm, bool persist, cudaStream_t st);
 
+// Per-shot data of a batch in device memory (see k_fused_tma_batch).
+template <typename T>
+struct BatchDev {
+  const StepArgs<T> *args;    // [2 * nshots]: index 2*s + parity of the step
+  const FusedExtras<T> *ext;  // [nshots] (it is set per launch)
+  const TmaMaps *maps;        // [2 * nshots]
+  const int *prefix;          // [nshots + 1] tile offsets in processing order
+  const int *order;           // [nshots] shot at each processing position
+  int nshots;
+  int *err;
+};
+
+template <typename T>
+int launch_fused_tma_batch(int kind, int nsls, const BatchDev<T> &b, int it, int nitems, int nsm,
+                           bool persist, cudaStream_t st);
+
+// Tensor maps of one ping-pong parity: the input state (in[0..4] = vx, vz,
+// sxx, szz, sxz; M with its plane stride) and the medium of `a`.
+template <typename T>
+int encode_parity(TmaMaps &m, const TmaBoxes &b, const vi_config &c, T *const in[5], const T *min,
+                  long long mstride, const StepArgs<T> &a);
+
 // Encodes a 2D (depth = 1) or 3D tensor map over an x-fastest array.
 int encode_map(CUtensorMap *map, const void *base, int esize, int nx, int nz, long long depth,
                long long plane_stride_elems, int box_x, int box_z, int box_d);

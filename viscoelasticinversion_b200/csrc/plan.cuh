@@ -41,4 +41,12 @@ int set_error(int code, const std::string &msg);
 int cuda_check(cudaError_t e, const char *what);
 // Grow-only device buffer.
 int ensure_buffer(vi_plan *p, void **buf, size_t *have, size_t need);
+// Step arguments of a plan for one medium and one set of fields (input side).
+template <typename T>
+StepArgs<T> make_args(const vi_plan *p, const vi_medium *m, const vi_fields *f);
+int check_medium(const vi_plan *p, const vi_medium *m);
+int check_fields(const vi_plan *p, const vi_fields *f);
+// Copies a shot's source / receiver lists to the plan's device buffers.
+template <typename T>
+int stage_shot(vi_plan *p, const vi_shot *s, cudaStream_t st);
 }  // namespace vb

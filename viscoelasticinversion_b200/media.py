@@ -14,6 +14,7 @@ outputs (planes of ρ, C and τ, and the τ_n of the mechanisms).
 """
 from __future__ import annotations
 
+import functools
 import math
 from dataclasses import dataclass, field
 
@@ -103,6 +104,7 @@ class QFit:
         return float(err.mean()), float(err.max())
 
 
+@functools.lru_cache(maxsize=64)
 def q_fit(f1: float, f2: float, N: int) -> QFit:
     """QModel(f1, f2, Nx, Nz, Q0, N) without the grids (Models.jl:90-102)."""
     w1, w2 = 2 * np.pi * f1, 2 * np.pi * f2
@@ -123,6 +125,27 @@ def thomsen_vti(vp, vs, rho, eps, delta):
     C11 = C33 * (1.0 + 2.0 * eps)
     C13 = np.sqrt(np.maximum((C33 - C55) * (C33 * (1.0 + 2.0 * delta) - C55), 0.0)) - C55
     return C11, C13, C33, C55
+
+
+def medium_from_velocity(kind, vp, vs, rho, eps=None, delta=None, Q=None, qfit=None) -> dict:
+    """Medium planes of vi_medium from (vp, vs, rho[, eps, delta], Q) fields:
+    ISO Lame (lambda in c13, mu in c55), VTI Thomsen (Models.jl:27-52), and
+    tau = N / (Kbar Q) of the Q fit (Models.jl:67) when qfit is given."""
+    vp, vs, rho = (np.asarray(a, dtype=np.float64) for a in (vp, vs, rho))
+    med = {"rho": rho.copy()}
+    if kind == "iso":
+        med["c13"] = rho * (vp**2 - 2 * vs**2)
+        med["c55"] = rho * vs**2
+    elif kind == "vti":
+        z = np.zeros_like(vp)
+        C11, C13, C33, C55 = thomsen_vti(vp, vs, rho, z if eps is None else eps,
+                                         z if delta is None else delta)
+        med.update(c11=C11, c13=C13, c33=C33, c55=C55)
+    else:
+        raise ValueError("medium_from_velocity: iso or vti")
+    if qfit is not None and len(qfit.taus):
+        med["tau"] = qfit.tau_for(np.broadcast_to(np.asarray(Q, dtype=np.float64), vp.shape)).copy()
+    return med
 
 
 def bond_rotate(C11, C13, C33, C55, theta):
@@ -328,7 +351,29 @@ def layered(nx=2048, nz=1024, dx=5.0, dt=0.4e-3, nt=4000, kind="vti", seed=0, nl
         sources=[(nx // 2, src_j, 0, 1.0)], wavelets=ricker_table(f0, 1.2 / f0, dt, nt)[None, :],
         receivers=_receiver_line(nx, pml, js + int(round(10.0 / dx)), nrec), vmax=vmax,
         meta={"f0": f0, "band": band, "eps": eps_l, "delta": del_l, "gamma": gam_l, "Q": q_l,
-              "theta": theta, "gamma_field": gamma, "seed": seed})
+              "theta": theta, "gamma_field": gamma, "seed": seed,
+              "fields": {"vp": vp, "vs": vs, "rho": rho, "eps": eps, "delta": dlt,
+                         "Q": np.broadcast_to(q_l[layer][:, None], shape).copy()}})
+
+
+GATHER_GRIDS = ((512, 512), (1024, 512), (1536, 768), (2048, 1024))
+
+
+def shot_gather(nshots: int = 64, seed: int = 0, kind: str = "tti", nt_range=(1500, 4000),
+                grids=GATHER_GRIDS, **kw) -> list:
+    """The batched workload: nshots shots, grid sizes drawn from
+    {512², 1024x512, 1536x768, 2048x1024}, nt uniform in [1500, 4000], each
+    a seeded layered medium (the 2048 x 1024 recipe) with a smooth tilt
+    field θ in ±30° for TTI.  Shot s uses medium seed 1000*seed + s."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(nshots):
+        nx, nz = grids[int(rng.integers(len(grids)))]
+        nt = int(rng.integers(nt_range[0], nt_range[1] + 1))
+        w = layered(nx=nx, nz=nz, nt=nt, kind=kind, seed=1000 * seed + s, **kw)
+        w.name = f"{kind}-gather{seed}-shot{s}-{nx}x{nz}-nt{nt}"
+        out.append(w)
+    return out
 
 
 def cfl_number(w: Workload) -> float:
