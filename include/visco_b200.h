@@ -177,6 +177,21 @@ int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);
 
+/* Same steps as vi_step with kernel_variant 1 (plain, in place), but it
+ * allocates no device memory: its strain planes and source/receiver lists
+ * live in one static device array of VI_NOALLOC_SCRATCH_BYTES per device
+ * and process.  No counterpart in the reference.  For callers
+ * that must not call cudaMalloc/cudaFree mid-run (a serving process sharing
+ * the GPU, whose allocations would synchronize it; a fully reserved HBM
+ * pool).  Limit: 6*nx*nz reals of the plan's precision plus the lists
+ * (<= 256 sources) must fit, else VI_ERR_ARG.  The first call on a device
+ * looks up the array's address; make it before any stream capture.  Each
+ * call clears the strain planes first.  Calls overlapping in time on one
+ * device race on the array: serialize them. */
+#define VI_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
+int vi_step_noalloc(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
+                    const vi_shot *shot, int32_t it0, int32_t nsteps, void *stream);
+
 /* One whole forward solve with host buffers: uploads the medium and the
  * wavelets, runs nt steps from a zero state and downloads the traces and
  * (optionally) the final wavefields.  Synchronous.  The end-to-end form of

@@ -109,6 +109,8 @@ _SIGNATURES = [
     ("vi_plan_last_kernel", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("vi_step", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.POINTER(ViFields),
                           C.POINTER(ViShot), C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    ("vi_step_noalloc", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.POINTER(ViFields),
+                                  C.POINTER(ViShot), C.c_int32, C.c_int32, C.c_void_p]),
     ("vi_forward_host", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.c_int32,
                                   C.POINTER(ViSource), C.c_void_p, C.c_int32,
                                   C.POINTER(ViReceiver), C.c_int32, C.c_void_p,
