@@ -19,7 +19,6 @@ struct SplitGeom {
       (int)(((long long)BW * BH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
   static constexpr int O0 = 128 / (int)sizeof(T);  // after the barrier slot
   static constexpr int BOX_BYTES = BW * BH * (int)sizeof(T);
-  static constexpr int SMEM_VEL = 128 + 3 * PB * (int)sizeof(T);
   static constexpr int SMEM_STRESS = 128 + 2 * PB * (int)sizeof(T);
 };
 
@@ -30,11 +29,11 @@ struct SplitMaps {
 };
 
 template <typename T>
-int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
-                     cudaStream_t st);
+int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, cudaStream_t st,
+                     bool pdl);
 template <typename T>
 int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
-                        const SplitMaps &m, int ntiles, cudaStream_t st);
+                        const SplitMaps &m, int ntiles, cudaStream_t st, bool pdl);
 
 // TMA maps of the pipelined split kernels: velocity (sxx, szz, sxz boxes,
 // vx, vz, rho tiles); stress (vx, vz boxes, sxx, szz, sxz tiles, M, then the
