@@ -99,8 +99,9 @@ def reduce_gradient(grad: torch.Tensor, misfit: float, group=None):
 
 
 def shot_gradient(gradient_fn, nshots: int, shape, device="cpu", group=None):
-    """Sum over shots of gradient_fn(i) -> (J_i, grad_i [8, nz, nx] float64),
-    each rank evaluating its shard and one all-reduce combining them."""
+    """(J, grad): the sum over shots of gradient_fn(i) -> (J_i, grad_i
+    [8, nz, nx] float64), each rank evaluating its shard and one all-reduce
+    combining them; every rank returns the full sum."""
     import torch.distributed as dist
 
     rank, world = 0, 1
@@ -112,4 +113,5 @@ def shot_gradient(gradient_fn, nshots: int, shape, device="cpu", group=None):
         Ji, gi = gradient_fn(i)
         total += gi
         J += Ji
-    return reduce_gradient(total, J, group)
+    total, J = reduce_gradient(total, J, group)
+    return J, total
