@@ -116,7 +116,8 @@ def measured_peaks():
 
 
 KERNEL_NAMES = {"fused-tma": "k_fused_tma", "fused-tma-1stage": "k_fused_tma", "fused": "k_fused",
-                "plain": "k_plain", "split": "k_split", "split-pipelined": "k_split_p"}
+                "plain": "k_plain", "split": "k_split", "split-pipelined": "k_split_p",
+                "stream": "k_stream"}
 KERNEL_PAIRS = {"split": "k_split_vel + k_split_stress",
                 "split-pipelined": "k_split_vel_p + k_split_stress_p"}
 

@@ -152,7 +152,7 @@ int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
 int vi_plan_status(vi_plan *plan, void *stream);
 /* Which kernel the last vi_step ran: 1 plain, 2 fused, 3 fused TMA-staged,
  * 4 fused TMA-staged single-stage, 5 split velocity/stress pair, 6 split
- * pair, persistent and TMA-pipelined. */
+ * pair, persistent and TMA-pipelined, 7 streaming. */
 int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
 
 /* ---- time stepping ------------------------------------------------------ */
@@ -171,8 +171,10 @@ int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
  * multi-kernel path (in place), 2 = fused kernel without TMA, 3 = TMA-staged
  * fused kernel (persistent, two stages when they fit), 4 = TMA-staged fused
  * kernel with one stage, 5 = split velocity/stress kernel pair (in place,
- * one tile per CTA), 6 = the split pair as persistent TMA-pipelined kernels.
- * Variants 3-6 return VI_ERR_ARG when not eligible. */
+ * one tile per CTA), 6 = the split pair as persistent TMA-pipelined kernels,
+ * 7 = streaming kernel (FP32 ISO/VTI: persistent CTAs march down 128-column
+ * strips with TMA row rings, one launch per step).
+ * Variants 3-7 return VI_ERR_ARG when not eligible. */
 int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);

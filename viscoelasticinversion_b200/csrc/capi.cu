@@ -8,6 +8,7 @@
 #include "plain.cuh"
 #include "plan.cuh"
 #include "split.cuh"
+#include "stream.cuh"
 
 namespace vb {
 
@@ -280,7 +281,7 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   rc = check_fields(p, f);
   if (rc) return rc;
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
-  if (variant < 0 || variant > 6) return set_error(VI_ERR_ARG, "unknown kernel variant");
+  if (variant < 0 || variant > 7) return set_error(VI_ERR_ARG, "unknown kernel variant");
   if (s && s->nrec > 0 && s->traces_nt > 0 && !s->traces_dev)
     return set_error(VI_ERR_ARG, "receivers need traces_dev");
   rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
@@ -318,6 +319,14 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     if (a.psix) a.psix = a.psix_o = (T *)p->psix + cur * kPsiPerSet * p->psix_plane;
     if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
     for (int k = 0; k < nsteps; ++k) plain_step<T>(a, x, p->cfg.medium, it0 + k, st);
+  } else if (variant == 7) {
+    if constexpr (sizeof(T) == 4) {
+      rc = stream_steps(p, a, s, it0, nsteps, st);
+      if (rc) return rc;
+      p->last_kernel = 7;
+    } else {
+      return set_error(VI_ERR_ARG, "the streaming step is FP32 only");
+    }
   } else if (variant == 5 || variant == 6 || (variant == 0 && split_eligible<T>(p, a))) {
     // the one-tile-per-CTA pair measures faster than the pipelined pair on
     // B200 (2048 x 1024 VTI: 27.6 vs 24.4 Gpt/s), so it is the default
