@@ -54,6 +54,10 @@ def parse_args():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--batch-shots", type=int, default=64)
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=40)
+    p.add_argument("--serve-explore", action="store_true",
+                   help="time several slice lengths and both scheduling policies")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     return p.parse_args()
 
@@ -273,6 +277,97 @@ def measure_batch(a, dev, stream, max_over_ranks, barrier, world):
     return out
 
 
+def measure_serving(a, dev, seed=0):
+    """Request serving on a bounded sample of the mixed request stream:
+    Poisson arrivals at 50 requests/s, 70 % forward / 30 % gradient, grids
+    from {256², 1024x512, 2048x1024, 4096x2048}, media from {iso, VTI, TTI}
+    (gradients: iso/VTI), step counts a quarter of [1000, 8000].  The same
+    arrivals are served twice: by the server with time slices given to the
+    request with the least remaining work (continuous batching) and FIFO one
+    request at a time with no slicing.  Slices are 1024 steps.
+    Latency = submit to results in host memory (ms)."""
+    import dataclasses
+    import threading
+
+    import numpy as np
+
+    from viscoelasticinversion_b200 import media
+    from viscoelasticinversion_b200.serve import Server
+
+    rng = np.random.default_rng(1234 + seed)
+    grids = ((256, 256), (1024, 512), (2048, 1024), (4096, 2048))
+    base = {}
+
+    def workload(g, kind):
+        if (g, kind) not in base:
+            base[(g, kind)] = media.layered(nx=g[0], nz=g[1], nt=2000, kind=kind, seed=7,
+                                            pml=20 if g[0] <= 256 else 40, nrec=64,
+                                            nlayers=4)
+        return base[(g, kind)]
+
+    n = a.serve_requests
+    reqs, t = [], 0.0
+    for _ in range(n):
+        t += rng.exponential(1 / 50.0)
+        grad = rng.random() < 0.3
+        kind = ("iso", "vti")[rng.integers(2)] if grad else ("iso", "vti", "tti")[rng.integers(3)]
+        g = grids[rng.integers(2)] if grad else grids[rng.integers(len(grids))]
+        if g == (4096, 2048) and kind == "tti":
+            kind = "vti"  # the tilt field of a 4096x2048 TTI medium takes ~15 s to generate
+        nt = int(rng.integers(250, 2001))
+        w0 = workload(g, kind)
+        w = dataclasses.replace(w0, nt=nt, wavelets=w0.wavelets[:, :nt])
+        reqs.append((t, grad, w))
+
+    def serve(slice_steps, max_active, policy):
+        srv = Server(device=dev.index, slice_steps=slice_steps, max_active=max_active, policy=policy)
+        tickets = []
+
+        def submitter():
+            t0 = time.perf_counter()
+            for at, grad, w in reqs:
+                d = at - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                obs = np.zeros((2, len(w.receivers), w.nt), np.float32)
+                tickets.append(srv.submit_gradient(w, obs, "f32") if grad else srv.submit_forward(w, "f32"))
+
+        t0 = time.perf_counter()
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for tk in tickets:
+            srv.wait(tk)
+        wall = time.perf_counter() - t0
+        lat = np.array([srv.poll(tk)[1] for tk in tickets])
+        srv.stop()
+        return lat, wall
+
+    # warm-up: one short request of every kind on every grid, so one-time
+    # kernel loading and set-up fall outside the timed runs
+    srv = Server(device=dev.index)
+    warm = []
+    for (g, kind), w0 in base.items():
+        w = dataclasses.replace(w0, nt=8, wavelets=w0.wavelets[:, :8])
+        warm.append(srv.submit_forward(w, "f32"))
+        if kind != "tti" and g[0] <= 1024:
+            warm.append(srv.submit_gradient(w, np.zeros((2, len(w.receivers), 8), np.float32), "f32"))
+    for tk in warm:
+        srv.wait(tk)
+    srv.stop()
+    pts = sum(w.nx * w.nz * w.nt * (3 if grad else 1) for _, grad, w in reqs)
+    out = {"workload": f"{n} requests, Poisson 50/s, 70% forward / 30% gradient, grids 256^2..4096x2048, "
+                       "iso/VTI/TTI (4096x2048: iso/VTI), nt 250..2000 (a quarter of 1000..8000), f32",
+           "forward": sum(1 for _, g, _ in reqs if not g), "gradient": sum(1 for _, g, _ in reqs if g)}
+    runs = [("sequential", (1 << 30, 1, "shortest-first"))] + [(n_, c) for n_, c in a.serve_policies]
+    for name, (sl, ma, pol) in runs:
+        lat, wall = serve(sl, ma, pol)
+        out[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "mean_ms": float(lat.mean()), "requests_per_s": n / wall, "wall_s": wall}
+    out["point_steps"] = pts
+    return out
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -411,6 +506,13 @@ def run_ours(a):
 
     if not a.no_batch:
         out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
+    if not a.no_serve and rank == 0 and world == 1:
+        a.serve_policies = [("continuous", (1024, 64, "shortest-first"))]
+        if a.serve_explore:
+            a.serve_policies += [("round-robin-256", (256, 64, "round-robin")),
+                                 ("shortest-first-256", (256, 64, "shortest-first")),
+                                 ("shortest-first-4096", (4096, 64, "shortest-first"))]
+        out["serving"] = measure_serving(a, dev)
     if rank == 0 and world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline(w, a.cpu_seconds)
     if rank == 0:

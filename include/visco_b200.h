@@ -262,6 +262,68 @@ int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const 
                          const double *vs, const double *rho, const double *eps,
                          const double *delta, double tau_scale, double *out4, void *stream);
 
+/* ---- request server ---------------------------------------------------- */
+/* Forward solves and misfit gradients submitted from any host thread and
+ * run by one worker thread on its own stream.  The reference solves one
+ * problem per call and has no server (ViscoelasticProblem.jl:273-309).
+ * Admission against an HBM budget; requests join and leave between slices
+ * of slice_steps steps (continuous batching), each slice going to the
+ * resident request with the least remaining work (cells x steps left), so
+ * short requests preempt long ones; gradient requests run whole.
+ * Every request has its own plan: its results equal a vi_forward_host /
+ * vi_gradient call on the same inputs, whatever else is resident. */
+typedef struct vi_server vi_server;
+typedef struct vi_serve_config {
+  int32_t device;
+  int32_t slice_steps;      /* steps per scheduling slice (<= 0: 1024) */
+  int32_t max_active;       /* requests resident at once (<= 0: 64) */
+  int32_t policy;           /* VI_SERVE_SHORTEST_FIRST or VI_SERVE_ROUND_ROBIN */
+  int64_t hbm_budget_bytes; /* device bytes the requests may hold (<= 0: 150 GB) */
+} vi_serve_config;
+
+#define VI_SERVE_SHORTEST_FIRST 0 /* each slice to the request with the least work left */
+#define VI_SERVE_ROUND_ROBIN 1    /* every resident request advances one slice per round */
+#define VI_REQ_FORWARD 0
+#define VI_REQ_GRADIENT 1
+#define VI_REQ_QUEUED 0
+#define VI_REQ_RUNNING 1
+#define VI_REQ_DONE 2
+#define VI_REQ_FAILED 3
+
+/* One request.  Host buffers are borrowed until the request is done or
+ * failed: medium planes (plan precision), wavelets (nsrc rows of
+ * wavelet_nt), the traces out ([2][nrec][nt]); for a gradient also the
+ * observed traces in, the FP64 gradient out ([8][nz][nx], vi_gradient's
+ * planes) and the misfit out.  Source and receiver lists are copied at
+ * submit. */
+typedef struct vi_request {
+  int32_t kind;             /* VI_REQ_FORWARD / VI_REQ_GRADIENT */
+  int32_t nt;
+  vi_config cfg;
+  vi_medium medium_host;
+  int32_t nsrc, wavelet_nt;
+  const vi_source *src_host;
+  const void *wavelet_host;
+  int32_t nrec, pad_;
+  const vi_receiver *rec_host;
+  void *traces_host;
+  const void *obs_host;
+  double *grad_host;
+  double *misfit_host;
+} vi_request;
+
+int vi_serve_start(const vi_serve_config *cfg, vi_server **out);
+/* Queues a request; VI_ERR_BUDGET when it could never fit the budget. */
+int vi_serve_submit(vi_server *server, const vi_request *req, uint64_t *ticket);
+/* Non-blocking: state (VI_REQ_*) and the latency so far or, when done,
+ * from submit to results in the host buffers; returns the request's error
+ * when it failed. */
+int vi_serve_poll(vi_server *server, uint64_t ticket, int32_t *state, double *latency_ms);
+/* Blocks until the request is done or failed, or timeout_s (< 0: no limit). */
+int vi_serve_wait(vi_server *server, uint64_t ticket, double timeout_s, int32_t *state);
+/* Finishes every queued and resident request, then frees the server. */
+int vi_serve_stop(vi_server *server);
+
 /* ---- staggered derivatives (diff-funcs.jl:3-32) ----------------------- */
 /* du = D(u) over the update region for one plane (device pointers, plan
  * precision).  op: 0 = ddxp, 1 = ddxm, 2 = ddzp, 3 = ddzm.  h is the grid

@@ -1,0 +1,112 @@
+"""The request server (vi_serve): every request's results equal the direct
+call on the same inputs, alone or in a mix of grids, media and step counts
+served in round-robin slices; gradients through the server equal
+vi_gradient; HBM-budget admission; failure reporting."""
+import numpy as np
+import pytest
+import torch
+
+from viscoelasticinversion_b200 import StepPlan, ViError, media
+from viscoelasticinversion_b200.gradient import misfit_gradient
+from viscoelasticinversion_b200.serve import Server
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix():
+    return [
+        media.homogeneous_iso(nx=96, nz=80, nt=150, pml=12, nrec=16, src=(40, 30)),
+        media.layered(nx=160, nz=96, nt=230, kind="vti", seed=1, pml=12, nrec=16),
+        media.layered(nx=128, nz=96, nt=170, kind="tti", seed=2, pml=12, nrec=16),
+        media.homogeneous_iso(nx=37, nz=29, nt=90, pml=6, nrec=7, src=(18, 14)),
+        media.layered(nx=136, nz=72, nt=201, kind="vti", seed=5, pml=10, nrec=12, nsls=1),
+    ]
+
+
+def _direct(w, precision):
+    plan = StepPlan.for_workload(w, precision)
+    tr = plan.forward_host(w.medium, w.sources, w.wavelets, w.receivers, w.nt)
+    plan.close()
+    return tr
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_forward_requests_equal_direct_calls(precision):
+    ws = _mix()
+    srv = Server(slice_steps=64)
+    tickets = [srv.submit_forward(w, precision) for w in ws]
+    for t in tickets:
+        assert srv.wait(t, 120.0) == "done"
+    for w, t in zip(ws, tickets):
+        state, lat = srv.poll(t)
+        assert state == "done" and lat > 0
+        assert np.array_equal(t.traces, _direct(w, precision)), w.name
+        assert np.abs(t.traces).max() > 0
+    srv.stop()
+
+
+def test_same_alone_and_in_the_mix():
+    ws = _mix()
+    srv = Server(slice_steps=50)
+    alone = srv.submit_forward(ws[1])
+    assert srv.wait(alone, 120.0) == "done"
+    mixed = [srv.submit_forward(w) for w in ws]
+    for t in mixed:
+        srv.wait(t, 120.0)
+    assert np.array_equal(alone.traces, mixed[1].traces)
+    srv.stop()
+
+
+def test_gradient_request_equals_vi_gradient(oracle_lib):
+    w = media.homogeneous_iso(nx=96, nz=80, nt=160, pml=12, nrec=16, src=(40, 30))
+    truth = dict(w.medium)
+    truth["c55"] = truth["c55"] * 1.03
+    import dataclasses
+    obs, _ = oracle_lib.run(dataclasses.replace(w, medium=truth), precision="f64")
+    srv = Server(slice_steps=64)
+    fwd = srv.submit_forward(w, "f64")
+    gt = srv.submit_gradient(w, obs, "f64")
+    assert srv.wait(gt, 120.0) == "done" and srv.wait(fwd, 120.0) == "done"
+    srv.stop()
+    plan = StepPlan.for_workload(w, "f64")
+    med = plan.medium_to_device(w.medium)
+    wav = torch.as_tensor(w.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
+    obs_d = torch.as_tensor(obs, dtype=plan.dtype, device=plan.device).contiguous()
+    J, g = misfit_gradient(plan, med, w.sources, wav, w.receivers, obs_d)
+    plan.close()
+    assert gt.misfit[0] == J
+    assert np.array_equal(gt.grad, g.cpu().numpy())
+    # the gradient's forward run (plain kernels) reproduces the forward solve
+    assert rel_l2(gt.traces, fwd.traces) <= 1e-12
+
+
+def test_budget_admission():
+    w = media.homogeneous_iso(nx=96, nz=80, nt=120, pml=12, nrec=8, src=(40, 30))
+    small = Server(hbm_budget_bytes=1 << 20)
+    with pytest.raises(ViError) as e:
+        small.submit_forward(w)
+    assert e.value.code == 3  # VI_ERR_BUDGET
+    small.stop()
+    # room for about one request at a time: all complete, one after another
+    one = Server(hbm_budget_bytes=25 << 20, slice_steps=30)
+    ts = [one.submit_forward(w) for _ in range(3)]
+    for t in ts:
+        assert one.wait(t, 120.0) == "done"
+    ref = _direct(w, "f32")
+    for t in ts:
+        assert np.array_equal(t.traces, ref)
+    one.stop()
+
+
+def test_failed_request_reports_error():
+    w = media.layered(nx=128, nz=64, nt=40, kind="tti", seed=1, pml=8, nrec=4)
+    srv = Server()
+    t = srv.submit_gradient(w, np.zeros((2, len(w.receivers), w.nt)), "f64")  # TTI has no gradient
+    with pytest.raises(ViError, match="TTI"):
+        srv.wait(t, 60.0)
+    with pytest.raises(ViError):
+        srv.poll(t)
+    ok = srv.submit_forward(w)  # the server keeps serving
+    assert srv.wait(ok, 60.0) == "done"
+    srv.stop()

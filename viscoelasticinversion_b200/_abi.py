@@ -79,6 +79,26 @@ class ViShot(C.Structure):
     ]
 
 
+class ViServeConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slice_steps", C.c_int32), ("max_active", C.c_int32),
+                ("policy", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
+class ViRequest(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("nt", C.c_int32), ("cfg", ViConfig), ("medium_host", ViMedium),
+        ("nsrc", C.c_int32), ("wavelet_nt", C.c_int32), ("src_host", C.POINTER(ViSource)),
+        ("wavelet_host", C.c_void_p), ("nrec", C.c_int32), ("pad_", C.c_int32),
+        ("rec_host", C.POINTER(ViReceiver)), ("traces_host", C.c_void_p), ("obs_host", C.c_void_p),
+        ("grad_host", C.c_void_p), ("misfit_host", C.c_void_p),
+    ]
+
+
+VI_SERVE_SHORTEST_FIRST, VI_SERVE_ROUND_ROBIN = 0, 1
+VI_REQ_FORWARD, VI_REQ_GRADIENT = 0, 1
+VI_REQ_QUEUED, VI_REQ_RUNNING, VI_REQ_DONE, VI_REQ_FAILED = 0, 1, 2, 3
+
+
 class ViError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -123,6 +143,11 @@ _SIGNATURES = [
                                     C.POINTER(ViFields), C.POINTER(ViShot), C.c_int32]),
     ("vi_batch_run", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     ("vi_batch_status", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    ("vi_serve_start", C.c_int, [C.POINTER(ViServeConfig), C.POINTER(C.c_void_p)]),
+    ("vi_serve_submit", C.c_int, [C.c_void_p, C.POINTER(ViRequest), C.POINTER(C.c_uint64)]),
+    ("vi_serve_poll", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    ("vi_serve_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_int32)]),
+    ("vi_serve_stop", C.c_int, [C.c_void_p]),
     ("vi_gradient", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.POINTER(ViShot), C.c_int32,
                               C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                               C.POINTER(C.c_double), C.c_void_p]),

@@ -1,0 +1,387 @@
+// serve.cu — a request server over the step: forward solves and misfit
+// gradients submitted from any host thread, run by one worker thread on its
+// own CUDA stream.
+//
+// The reference solves one problem per call and has no server
+// (sciml_solver/ViscoelasticProblem.jl:273-309).  Scheduling here:
+//  * admission: a request is admitted when its device footprint (estimated
+//    from its grid, mechanisms, precision and step count) fits the HBM
+//    budget next to the requests already resident; one that could never
+//    fit is refused at submit (VI_ERR_BUDGET);
+//  * continuous batching by time slices: requests join and leave between
+//    slices of slice_steps steps; each slice goes to the resident request
+//    with the least remaining work (grid cells x steps left, x3 for a
+//    gradient), so a short request that arrives while a long one runs
+//    preempts it at the next slice boundary (shortest remaining work
+//    first, which minimises mean latency);
+//  * gradient requests run whole when their turn comes (one vi_gradient).
+// Each request has its own plan and device buffers, so its results do not
+// depend on what else is resident (the sliced stepping is bitwise equal to
+// one vi_step call).  Latency is measured from submit to the moment the
+// results are in the caller's host buffers.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "plan.cuh"
+
+using Clock = std::chrono::steady_clock;
+
+namespace vb {
+namespace {
+
+struct Req {
+  uint64_t ticket = 0;
+  vi_request rq{};
+  std::vector<vi_source> src;
+  std::vector<vi_receiver> rec;
+  int state = VI_REQ_QUEUED;
+  int err = VI_OK;
+  std::string msg;
+  Clock::time_point t_submit, t_done;
+  int64_t footprint = 0;
+  // resident state (worker thread only)
+  vi_plan *plan = nullptr;
+  void *buf = nullptr;
+  vi_medium md{};
+  vi_fields fd{};
+  vi_shot shot{};
+  void *obs_dev = nullptr;
+  double *grad_dev = nullptr;
+  int done_steps = 0;
+};
+
+size_t esize_of(const vi_config &c) { return c.precision == VI_F64 ? 8 : 4; }
+
+// Remaining work of a request in grid-cell steps (the scheduling key; a
+// gradient costs about three forward passes, a TTI step about two).
+double remaining_work(const Req &q) {
+  const vi_request &r = q.rq;
+  const double cells = (double)r.cfg.nx * r.cfg.nz;
+  const double left = (double)(r.nt - q.done_steps);
+  return cells * left * (r.kind == VI_REQ_GRADIENT ? 3.0 : 1.0) * (r.cfg.medium == VI_MEDIUM_TTI ? 2.0 : 1.0);
+}
+
+// Device bytes a request holds while resident (plan workspace included,
+// rounded up): medium, state, the fused path's second state copy, CPML
+// strips, wavelets and traces; for a gradient the checkpoints and segment
+// slots, the adjoint state and scratch, observed traces and FP64 planes.
+int64_t footprint(const vi_request &r) {
+  const vi_config &c = r.cfg;
+  const int64_t np = (int64_t)c.nx * c.nz, e = (int64_t)esize_of(c);
+  const int64_t ns = 5 + 3 * (int64_t)c.nsls;
+  const int64_t pml = c.pml_thickness > 0 ? c.pml_thickness : 0;
+  const int64_t psi = 2 * 4 * (2 * pml * c.nz + c.nx * 2 * pml) * e;
+  const int64_t tr = 2 * (int64_t)r.nrec * r.nt * e;
+  const int64_t wav = (int64_t)r.nsrc * (r.wavelet_nt > 0 ? r.wavelet_nt : 0) * e;
+  int64_t b = (8 + 2 * ns + 6) * np * e + psi + 2 * tr + wav + (16 << 20);
+  if (r.kind == VI_REQ_GRADIENT) {
+    int64_t K = 1;
+    while (K * K < r.nt) ++K;
+    const int64_t nck = (r.nt + K - 1) / K;
+    const int64_t slot = ns * np * e + psi / 2;
+    b += (nck + K + 2) * slot + 13 * np * e + 8 * np * 8 + tr;
+  }
+  return b;
+}
+
+}  // namespace
+}  // namespace vb
+
+using namespace vb;
+
+struct vi_server {
+  vi_serve_config cfg{};
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::shared_ptr<Req>> queue;
+  std::vector<std::shared_ptr<Req>> active;
+  std::unordered_map<uint64_t, std::shared_ptr<Req>> all;
+  uint64_t next_ticket = 1;
+  bool stopping = false;
+  int64_t used = 0;
+  cudaStream_t st = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int admit_impl(vi_server *s, Req &q) {
+  const vi_request &r = q.rq;
+  const vi_config &c = r.cfg;
+  const size_t np = (size_t)c.nx * c.nz;
+  int rc = vi_plan_create(&c, &q.plan);
+  if (rc) return rc;
+  const int ns = 5 + 3 * c.nsls;
+  const int nmed = 8;
+  const size_t tr = 2 * (size_t)r.nrec * r.nt;
+  const size_t wav = (size_t)r.nsrc * (r.wavelet_nt > 0 ? r.wavelet_nt : 0);
+  const bool grad = r.kind == VI_REQ_GRADIENT;
+  size_t elems = (nmed + ns) * np + wav + tr + (grad ? tr : 0) + 64;
+  size_t bytes = elems * sizeof(T) + (grad ? 8 * np * sizeof(double) + 256 : 0);
+  if ((rc = cuda_check(cudaMalloc(&q.buf, bytes), "serve: allocate request buffers"))) return rc;
+  T *base = (T *)q.buf;
+  const void *hp[8] = {r.medium_host.rho, r.medium_host.c11, r.medium_host.c13, r.medium_host.c15,
+                       r.medium_host.c33, r.medium_host.c35, r.medium_host.c55, r.medium_host.tau};
+  const void **dp[8] = {&q.md.rho, &q.md.c11, &q.md.c13, &q.md.c15, &q.md.c33, &q.md.c35, &q.md.c55, &q.md.tau};
+  for (int k = 0; k < 8; ++k) {
+    *dp[k] = nullptr;
+    if (hp[k]) {
+      T *d = base + k * np;
+      if ((rc = cuda_check(cudaMemcpyAsync(d, hp[k], np * sizeof(T), cudaMemcpyHostToDevice, s->st),
+                           "serve: upload medium")))
+        return rc;
+      *dp[k] = d;
+    }
+  }
+  T *state = base + nmed * np;
+  if ((rc = cuda_check(cudaMemsetAsync(state, 0, ns * np * sizeof(T), s->st), "serve: zero state"))) return rc;
+  q.fd.vx = state;
+  q.fd.vz = state + np;
+  q.fd.sxx = state + 2 * np;
+  q.fd.szz = state + 3 * np;
+  q.fd.sxz = state + 4 * np;
+  q.fd.m = c.nsls ? state + 5 * np : nullptr;
+  q.fd.m_plane_stride = (long long)np;
+  T *w = state + ns * np;
+  T *t = w + wav;
+  if (wav && (rc = cuda_check(cudaMemcpyAsync(w, r.wavelet_host, wav * sizeof(T), cudaMemcpyHostToDevice, s->st),
+                              "serve: upload wavelets")))
+    return rc;
+  if (tr && (rc = cuda_check(cudaMemsetAsync(t, 0, tr * sizeof(T), s->st), "serve: zero traces"))) return rc;
+  if (grad) {
+    T *o = t + tr;
+    if ((rc = cuda_check(cudaMemcpyAsync(o, r.obs_host, tr * sizeof(T), cudaMemcpyHostToDevice, s->st),
+                         "serve: upload observed traces")))
+      return rc;
+    q.obs_dev = o;
+    uintptr_t gp = ((uintptr_t)(o + tr) + 255) / 256 * 256;
+    q.grad_dev = (double *)gp;
+  }
+  q.shot.nsrc = r.nsrc;
+  q.shot.src_host = q.src.empty() ? nullptr : q.src.data();
+  q.shot.wavelet_dev = w;
+  q.shot.wavelet_nt = r.wavelet_nt;
+  q.shot.nrec = r.nrec;
+  q.shot.rec_host = q.rec.empty() ? nullptr : q.rec.data();
+  q.shot.traces_dev = t;
+  q.shot.traces_nt = r.nt;
+  if ((rc = vi_plan_reset(q.plan, s->st))) return rc;
+  return cuda_check(cudaStreamSynchronize(s->st), "serve: stage request");
+}
+
+int admit(vi_server *s, Req &q) {
+  return q.rq.cfg.precision == VI_F64 ? admit_impl<double>(s, q) : admit_impl<float>(s, q);
+}
+
+void release(Req &q) {
+  if (q.plan) vi_plan_destroy(q.plan);
+  q.plan = nullptr;
+  if (q.buf) cudaFree(q.buf);
+  q.buf = nullptr;
+}
+
+// Runs the request's next slice (forward) or all of it (gradient); returns
+// true when the request is finished.
+int advance(vi_server *s, Req &q, bool *finished) {
+  const vi_request &r = q.rq;
+  const size_t es = esize_of(r.cfg);
+  int rc;
+  if (r.kind == VI_REQ_GRADIENT) {
+    double J = 0;
+    if ((rc = vi_gradient(q.plan, &q.md, &q.shot, r.nt, q.obs_dev, 0, 0, q.grad_dev, &J, s->st))) return rc;
+    const size_t np = (size_t)r.cfg.nx * r.cfg.nz;
+    if ((rc = cuda_check(cudaMemcpyAsync(r.grad_host, q.grad_dev, 8 * np * sizeof(double), cudaMemcpyDeviceToHost,
+                                         s->st),
+                         "serve: download gradient")))
+      return rc;
+    if (r.misfit_host) *r.misfit_host = J;
+  } else {
+    int n = s->cfg.slice_steps;
+    if (n > r.nt - q.done_steps) n = r.nt - q.done_steps;
+    if ((rc = vi_step(q.plan, &q.md, &q.fd, &q.shot, q.done_steps, n, 0, s->st))) return rc;
+    q.done_steps += n;
+    if (q.done_steps < r.nt) {
+      *finished = false;
+      return VI_OK;
+    }
+    if ((rc = vi_plan_status(q.plan, s->st))) return rc;
+  }
+  const size_t tr = 2 * (size_t)r.nrec * r.nt;
+  if (tr && r.traces_host &&
+      (rc = cuda_check(cudaMemcpyAsync(r.traces_host, q.shot.traces_dev, tr * es, cudaMemcpyDeviceToHost, s->st),
+                       "serve: download traces")))
+    return rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(s->st), "serve: finish request"))) return rc;
+  *finished = true;
+  return VI_OK;
+}
+
+void finish(vi_server *s, const std::shared_ptr<Req> &q, int rc) {
+  release(*q);
+  std::lock_guard<std::mutex> lk(s->mu);
+  q->err = rc;
+  if (rc) q->msg = vi_last_error();
+  q->state = rc ? VI_REQ_FAILED : VI_REQ_DONE;
+  q->t_done = Clock::now();
+  s->used -= q->footprint;
+  s->cv.notify_all();
+}
+
+void worker_main(vi_server *s) {
+  cudaSetDevice(s->cfg.device);
+  for (;;) {
+    std::vector<std::shared_ptr<Req>> admitted;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      // wait for work unless requests are resident
+      s->cv.wait(lk, [&] { return s->stopping || !s->queue.empty() || !s->active.empty(); });
+      while (!s->queue.empty() && (int)s->active.size() + (int)admitted.size() < s->cfg.max_active &&
+             s->used + s->queue.front()->footprint <= s->cfg.hbm_budget_bytes) {
+        auto q = s->queue.front();
+        s->queue.pop_front();
+        s->used += q->footprint;
+        q->state = VI_REQ_RUNNING;
+        admitted.push_back(q);
+      }
+      if (s->stopping && s->queue.empty() && s->active.empty() && admitted.empty()) return;
+    }
+    for (auto &q : admitted) {
+      const int rc = admit(s, *q);
+      if (rc) {
+        finish(s, q, rc);
+        continue;
+      }
+      s->active.push_back(q);  // worker-owned list
+    }
+    if (s->active.empty()) continue;
+    std::vector<std::shared_ptr<Req>> picks;
+    if (s->cfg.policy == VI_SERVE_ROUND_ROBIN) {
+      picks = s->active;  // one slice each
+    } else {  // one slice for the resident request with the least remaining work
+      size_t best = 0;
+      for (size_t k = 1; k < s->active.size(); ++k)
+        if (remaining_work(*s->active[k]) < remaining_work(*s->active[best])) best = k;
+      picks.push_back(s->active[best]);
+    }
+    for (auto &q : picks) {
+      bool fin = false;
+      const int rc = advance(s, *q, &fin);
+      if (rc || fin) {
+        finish(s, q, rc);
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (size_t k = 0; k < s->active.size(); ++k)
+          if (s->active[k] == q) {
+            s->active.erase(s->active.begin() + (long)k);
+            break;
+          }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int vi_serve_start(const vi_serve_config *cfg, vi_server **out) {
+  if (!cfg || !out) return set_error(VI_ERR_ARG, "serve: NULL argument");
+  int ndev = 0;
+  int rc = cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (rc) return rc;
+  if (cfg->device < 0 || cfg->device >= ndev) return set_error(VI_ERR_ARG, "serve: no such device");
+  auto *s = new vi_server();
+  s->cfg = *cfg;
+  if (s->cfg.slice_steps <= 0) s->cfg.slice_steps = 1024;
+  if (s->cfg.max_active <= 0) s->cfg.max_active = 64;
+  if (s->cfg.hbm_budget_bytes <= 0) s->cfg.hbm_budget_bytes = 150LL * 1000 * 1000 * 1000;
+  if (s->cfg.policy != VI_SERVE_ROUND_ROBIN) s->cfg.policy = VI_SERVE_SHORTEST_FIRST;
+  if ((rc = cuda_check(cudaSetDevice(cfg->device), "cudaSetDevice")) ||
+      (rc = cuda_check(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "serve: create stream"))) {
+    delete s;
+    return rc;
+  }
+  s->worker = std::thread(worker_main, s);
+  *out = s;
+  return VI_OK;
+}
+
+extern "C" int vi_serve_submit(vi_server *s, const vi_request *r, uint64_t *ticket) {
+  if (!s || !r || !ticket) return set_error(VI_ERR_ARG, "serve: NULL argument");
+  if (r->kind != VI_REQ_FORWARD && r->kind != VI_REQ_GRADIENT) return set_error(VI_ERR_ARG, "serve: unknown request kind");
+  if (r->nt <= 0) return set_error(VI_ERR_ARG, "serve: nt must be positive");
+  if (r->nsrc < 0 || r->nrec < 0) return set_error(VI_ERR_ARG, "serve: negative source/receiver count");
+  if (r->nsrc > 0 && (!r->src_host || !r->wavelet_host || r->wavelet_nt <= 0))
+    return set_error(VI_ERR_ARG, "serve: sources need src_host and wavelet_host");
+  if (r->nrec > 0 && (!r->rec_host || !r->traces_host)) return set_error(VI_ERR_ARG, "serve: receivers need rec_host and traces_host");
+  if (r->kind == VI_REQ_GRADIENT && (!r->obs_host || !r->grad_host || r->nrec <= 0))
+    return set_error(VI_ERR_ARG, "serve: gradient requests need receivers, obs_host and grad_host");
+  if (!r->medium_host.rho) return set_error(VI_ERR_ARG, "serve: medium_host is incomplete");
+  auto q = std::make_shared<Req>();
+  q->rq = *r;
+  q->src.assign(r->src_host, r->src_host + r->nsrc);
+  q->rec.assign(r->rec_host, r->rec_host + r->nrec);
+  q->footprint = footprint(*r);
+  if (q->footprint > s->cfg.hbm_budget_bytes)
+    return set_error(VI_ERR_BUDGET, "serve: request needs " + std::to_string(q->footprint) +
+                                        " device bytes, more than the budget " +
+                                        std::to_string(s->cfg.hbm_budget_bytes));
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stopping) return set_error(VI_ERR_STATE, "serve: server is stopping");
+  q->ticket = s->next_ticket++;
+  q->t_submit = Clock::now();
+  s->all[q->ticket] = q;
+  s->queue.push_back(q);
+  *ticket = q->ticket;
+  s->cv.notify_all();
+  return VI_OK;
+}
+
+extern "C" int vi_serve_poll(vi_server *s, uint64_t ticket, int32_t *state, double *latency_ms) {
+  if (!s || !state) return set_error(VI_ERR_ARG, "serve: NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return set_error(VI_ERR_ARG, "serve: unknown ticket");
+  const Req &q = *it->second;
+  *state = q.state;
+  const auto end = (q.state == VI_REQ_DONE || q.state == VI_REQ_FAILED) ? q.t_done : Clock::now();
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(end - q.t_submit).count();
+  if (q.state == VI_REQ_FAILED) return set_error(q.err, "serve: request failed: " + q.msg);
+  return VI_OK;
+}
+
+extern "C" int vi_serve_wait(vi_server *s, uint64_t ticket, double timeout_s, int32_t *state) {
+  if (!s || !state) return set_error(VI_ERR_ARG, "serve: NULL argument");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return set_error(VI_ERR_ARG, "serve: unknown ticket");
+  auto q = it->second;
+  auto done = [&] { return q->state == VI_REQ_DONE || q->state == VI_REQ_FAILED; };
+  if (timeout_s < 0)
+    s->cv.wait(lk, done);
+  else
+    s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
+  *state = q->state;
+  if (q->state == VI_REQ_FAILED) return set_error(q->err, "serve: request failed: " + q->msg);
+  return VI_OK;
+}
+
+extern "C" int vi_serve_stop(vi_server *s) {
+  if (!s) return set_error(VI_ERR_ARG, "serve: NULL argument");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+    s->cv.notify_all();
+  }
+  if (s->worker.joinable()) s->worker.join();
+  cudaSetDevice(s->cfg.device);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return VI_OK;
+}
