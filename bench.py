@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--batch-shots", type=int, default=64)
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-grad", action="store_true")
+    p.add_argument("--grad-nt", type=int, default=3000)
     p.add_argument("--serve-requests", type=int, default=40)
     p.add_argument("--serve-explore", action="store_true",
                    help="time several slice lengths and both scheduling policies")
@@ -368,6 +370,47 @@ def measure_serving(a, dev, seed=0):
     return out
 
 
+def measure_gradient(a, dev):
+    """Misfit gradient of one shot of the 1024 x 512, 3000-step FP32 VTI
+    gradient workload (C2 recipe, start model Gaussian-smoothed with
+    sigma = 100 m, observed traces from the true model), through
+    vi_gradient: seconds, grid-point steps per second of the whole gradient
+    (forward + recompute + adjoint), and the misfit."""
+    import numpy as np
+    import torch
+    from scipy.ndimage import gaussian_filter
+
+    from viscoelasticinversion_b200 import StepPlan, media
+    from viscoelasticinversion_b200.gradient import misfit_gradient
+
+    true = media.layered(nx=1024, nz=512, nt=a.grad_nt, kind="vti", seed=3)
+    start = dict(true.medium)
+    for k in start:
+        start[k] = gaussian_filter(true.medium[k], 100.0 / true.dx, mode="nearest")
+    plan = StepPlan.for_workload(true, "f32", device=dev.index)
+    wav = torch.as_tensor(true.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
+    obs = torch.zeros(2, len(true.receivers), true.nt, dtype=plan.dtype, device=plan.device)
+    med_t = plan.medium_to_device(true.medium)
+    st = plan.zeros_state()
+    plan.reset()
+    plan.step(med_t, st, nsteps=true.nt, sources=true.sources, wavelets=wav,
+              receivers=true.receivers, traces=obs)
+    plan.status()
+    med = plan.medium_to_device(start)
+    nw = min(true.nt, 50)
+    misfit_gradient(plan, med, true.sources, wav, true.receivers, obs[:, :, :nw].contiguous(), nt=nw)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, g = misfit_gradient(plan, med, true.sources, wav, true.receivers, obs)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    plan.close()
+    pts = true.nx * true.nz * true.nt
+    return {"workload": f"vti-1024x512-nt{true.nt}-f32-gradient (start model smoothed 100 m)",
+            "seconds": sec, "gpts": pts / sec / 1e9, "misfit": J,
+            "grad_finite": bool(torch.isfinite(g).all().item())}
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -506,6 +549,8 @@ def run_ours(a):
 
     if not a.no_batch:
         out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
+    if not a.no_grad and rank == 0:
+        out["gradient"] = measure_gradient(a, dev)
     if not a.no_serve and rank == 0 and world == 1:
         a.serve_policies = [("continuous", (1024, 64, "shortest-first"))]
         if a.serve_explore:
