@@ -27,8 +27,11 @@
 #include <cmath>
 #include <vector>
 
+#include "fused.cuh"
+#include "fused_tma.cuh"
 #include "plain.cuh"
 #include "plan.cuh"
+#include "split.cuh"
 
 namespace vb {
 
@@ -61,8 +64,10 @@ struct Slot {
   __host__ __device__ T *m() const { return base + 5 * np; }
   __host__ __device__ T *psix() const { return base + (5 + 3 * nsls) * np; }
   __host__ __device__ T *psiz() const { return psix() + 4 * px; }
+  // rounded up to 64 elements, so every slot (and, with nx % 4 == 0, every
+  // plane of it) starts on a 16-byte boundary, as the split kernels need
   __host__ __device__ static long long size(long long np, long long px, long long pz, int nsls) {
-    return (5 + 3 * nsls) * np + 4 * px + 4 * pz;
+    return ((5 + 3 * nsls) * np + 4 * px + 4 * pz + 63) / 64 * 64;
   }
 };
 
@@ -503,19 +508,64 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   const size_t sbytes = (size_t)slot * sizeof(T);
   // plain-path scratch: cells outside the update region are read, never written
   if ((rc = cuda_check(cudaMemsetAsync(pscr, 0, 6 * np * sizeof(T), st), "zero scratch"))) return rc;
+  // The two forward sweeps (traces + checkpoints, then the segment
+  // recompute) run on the split pair when the grid allows it (the same
+  // discrete step as the plain path the adjoint transposes, faster), else
+  // on the plain path.
+  using SG = SplitGeom<T>;
+  StepArgs<T> probe = a;
+  bind(probe, mk(seg));
+  const bool use_split = split_eligible<T>(p, probe);
+  FusedExtras<T> fx{};
+  SplitMaps ms{};
+  int ntiles = 0;
+  if (use_split) {
+    int ntx = 0, ntz = 0;
+    std::vector<int> off;
+    std::vector<int4> ent;
+    build_tile_lists(c.nx, c.nz, SG::TX, SG::TZ, 0, shot, off, ent, ntx, ntz);
+    int *d_off = nullptr;
+    int4 *d_ent = nullptr;
+    if ((rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent))) return rc;
+    ntiles = ntx * ntz;
+    fx.ntx = ntx;
+    fx.fs = c.free_surface;
+    fx.tile_off = d_off;
+    fx.tile_ent = d_ent;
+    fx.amp = (const T *)p->damp;
+    fx.wavelet = shot->nsrc ? (const T *)shot->wavelet_dev : nullptr;
+    fx.wnt = shot->nsrc ? shot->wavelet_nt : 0;
+    fx.nrec = nrec;
+    fx.tnt = nt;
+    fx.err = (int *)p->errflag;
+  }
+  auto fwd_step = [&](const Slot<T> &sl, int it, T *traces, bool pdl) -> int {
+    if (!use_split) {
+      bind(a, sl);
+      x.traces = traces;
+      plain_step<T>(a, x, c.medium, it, st);
+      return VI_OK;
+    }
+    StepArgs<T> b = a;
+    bind(b, sl);
+    fx.it = it;
+    fx.traces = traces;
+    int r2 = encode_map(&ms.a, b.vx, (int)sizeof(T), c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1);
+    if (!r2) r2 = encode_map(&ms.b, b.vz, (int)sizeof(T), c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1);
+    if (!r2) r2 = launch_split_vel<T>(b, fx, ntiles, st, pdl);
+    if (!r2) r2 = launch_split_stress<T>(c.medium, b, fx, ms, ntiles, st, true);
+    return r2;
+  };
   // ---- forward sweep with checkpoints and traces ----
   Slot<T> cur = mk(seg);
   if ((rc = cuda_check(cudaMemsetAsync(seg, 0, sbytes, st), "zero state"))) return rc;
-  bind(a, cur);
-  x.traces = tr;
   for (int it = 0; it < nt; ++it) {
     if (it % K == 0)
       if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, seg, sbytes, cudaMemcpyDeviceToDevice, st),
                            "checkpoint")))
         return rc;
-    plain_step<T>(a, x, c.medium, it, st);
+    if ((rc = fwd_step(cur, it, tr, it % K != 0))) return rc;
   }
-  x.traces = nullptr;
   if (shot->traces_dev && shot->traces_nt >= nt) {
     for (int k = 0; k < 2 * nrec; ++k)
       cudaMemcpyAsync((T *)shot->traces_dev + (size_t)k * shot->traces_nt, tr + (size_t)k * nt,
@@ -562,8 +612,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
       if ((rc = cuda_check(cudaMemcpyAsync(nxt, seg + (size_t)k * slot, sbytes, cudaMemcpyDeviceToDevice, st),
                            "segment copy")))
         return rc;
-      bind(a, mk(nxt));
-      plain_step<T>(a, x, c.medium, s0 + k, st);
+      if ((rc = fwd_step(mk(nxt), s0 + k, nullptr, false))) return rc;
     }
     for (int it = s1 - 1; it >= s0; --it) {
       const Slot<T> x0 = mk(seg + (size_t)(it - s0) * slot), x1 = mk(seg + (size_t)(it - s0 + 1) * slot);
