@@ -211,95 +211,89 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 2 : 1)
   T hvx[12], hvz[12];
   row12s(s_vx + vb, hvx);
   row12s(s_vz + vb, hvz);
-  T zvz[4] = {0, 0, 0, 0}, zvx[4] = {0, 0, 0, 0};
+  Q4<T> zvz = splat4<T>(0), zvx = splat4<T>(0);
 #pragma unroll
   for (int q = -4; q <= 4; ++q) {
     if (q <= 3) {  // ddzm(vz)
       const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
-      const Q4<T> v = q == 0 ? Q4<T>{{hvz[4], hvz[5], hvz[6], hvz[7]}} : lds4(s_vz + vb + q * SW + 4);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) zvz[k] += cq * v.v[k];
+      const Q4<T> v = q == 0 ? win4(hvz, 4) : lds4(s_vz + vb + q * SW + 4);
+      zvz = fma4(splat4<T>(cq), v, zvz);
     }
     if (q >= -3) {  // ddzp(vx)
       const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
-      const Q4<T> v = q == 0 ? Q4<T>{{hvx[4], hvx[5], hvx[6], hvx[7]}} : lds4(s_vx + vb + q * SW + 4);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) zvx[k] += cq * v.v[k];
+      const Q4<T> v = q == 0 ? win4(hvx, 4) : lds4(s_vx + vb + q * SW + 4);
+      zvx = fma4(splat4<T>(cq), v, zvx);
     }
   }
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
   const bool surf = x.fs && gj == L;
-  T rxx[4], rzz[4], rxz[4];
+  Q4<T> rxx = dms4(hvx, a.Dx), dxvz = dps4(hvz, a.Dx), rzz = zvz, dzvx = zvx;
+  if (xstrip) {  // CPML, cell by cell
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int gi = gi0 + k;
-    T dxvx = dms(hvx, 4 + k, a.Dx), dxvz = dps(hvz, 4 + k, a.Dx);
-    T dzvz = zvz[k], dzvx = zvx[k];
-    if (xstrip) {
+    for (int k = 0; k < 4; ++k) {
+      const int gi = gi0 + k;
       const int xs = strip_x(gi, nx, a.Lx, a.Rx);
       if (xs >= 0) {
         const T *tb = a.tx;
         const long long o = (long long)gj * a.wx + xs;
         T *p0 = a.psix + PX_VX * a.psix_plane + o, *p1 = a.psix + PX_VZ * a.psix_plane + o;
-        *p0 = tb[T_B * nx + gi] * *p0 + tb[T_A * nx + gi] * dxvx;
-        *p1 = tb[T_BH * nx + gi] * *p1 + tb[T_AH * nx + gi] * dxvz;
-        dxvx = dxvx * tb[T_IK * nx + gi] + *p0;
-        dxvz = dxvz * tb[T_IKH * nx + gi] + *p1;
+        *p0 = tb[T_B * nx + gi] * *p0 + tb[T_A * nx + gi] * rxx.v[k];
+        *p1 = tb[T_BH * nx + gi] * *p1 + tb[T_AH * nx + gi] * dxvz.v[k];
+        rxx.v[k] = rxx.v[k] * tb[T_IK * nx + gi] + *p0;
+        dxvz.v[k] = dxvz.v[k] * tb[T_IKH * nx + gi] + *p1;
       }
     }
-    if (zs >= 0) {
-      const T *tb = a.tz;
-      const long long o = (long long)zs * nx + gi;
+  }
+  if (zs >= 0) {
+    const T *tb = a.tz;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long o = (long long)zs * nx + gi0 + k;
       T *p0 = a.psiz + PZ_VZ * a.psiz_plane + o, *p1 = a.psiz + PZ_VX * a.psiz_plane + o;
-      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * dzvz;
-      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * dzvx;
-      dzvz = dzvz * tb[T_IK * nz + gj] + *p0;
-      dzvx = dzvx * tb[T_IKH * nz + gj] + *p1;
+      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * rzz.v[k];
+      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * dzvx.v[k];
+      rzz.v[k] = rzz.v[k] * tb[T_IK * nz + gj] + *p0;
+      dzvx.v[k] = dzvx.v[k] * tb[T_IKH * nz + gj] + *p1;
     }
-    rxx[k] = dxvx;
-    rzz[k] = dzvz;
-    rxz[k] = dzvx + dxvz;
   }
-  // ---- SLS effective rates and the stress update
+  const Q4<T> rxz = add4(dzvx, dxvz);
+  // ---- SLS effective rates and the stress update (4 cells at once)
   const T dt = a.dt;
+  const Q4<T> dt4 = splat4<T>(dt);
+  Q4<T> exx = rxx, ezz = rzz, exz = rxz;
+  if constexpr (NSLS > 0) {
+    Q4<T> Sxx = m[0], Szz = m[NSLS], Sxz = m[2 * NSLS];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    T exx = rxx[k], ezz = rzz[k], exz = rxz[k];
-    if constexpr (NSLS > 0) {
-      T Sxx = 0, Szz = 0, Sxz = 0;
-#pragma unroll
-      for (int n = 0; n < NSLS; ++n) {
-        Sxx += m[0 * NSLS + n].v[k];
-        Szz += m[1 * NSLS + n].v[k];
-        Sxz += m[2 * NSLS + n].v[k];
-      }
-      const T t = tau.v[k], t1 = T(1) + t;
-      exx = t1 * rxx[k] + t * Sxx;
-      ezz = t1 * rzz[k] + t * Szz;
-      exz = t1 * rxz[k] + t * Sxz;
+    for (int n = 1; n < NSLS; ++n) {
+      Sxx = add4(Sxx, m[0 * NSLS + n]);
+      Szz = add4(Szz, m[1 * NSLS + n]);
+      Sxz = add4(Sxz, m[2 * NSLS + n]);
     }
-    const T C13 = c13.v[k];
-    const T C11 = KIND == VI_MEDIUM_ISO ? C13 + T(2) * c55a.v[k] : c11.v[k];
-    const T C33 = KIND == VI_MEDIUM_ISO ? C11 : c33.v[k];
-    if (surf) ezz = -(C13 * exx) / C33;
-    const T c55r = k < 3 ? c55a.v[k + 1] : c55a4, c55br = k < 3 ? c55b.v[k + 1] : c55b4;
-    const T C55h = T(0.25) * (c55a.v[k] + c55r + c55b.v[k] + c55br);
-    sxx.v[k] += dt * (C11 * exx + C13 * ezz);
-    szz.v[k] += dt * (C13 * exx + C33 * ezz);
-    sxz.v[k] += dt * (C55h * exz);
+    const Q4<T> t1 = add4(tau, splat4<T>(T(1)));
+    exx = fma4(t1, rxx, mul4(tau, Sxx));
+    ezz = fma4(t1, rzz, mul4(tau, Szz));
+    exz = fma4(t1, rxz, mul4(tau, Sxz));
   }
+  const Q4<T> C13 = c13;
+  const Q4<T> C11 = KIND == VI_MEDIUM_ISO ? fma4(splat4<T>(T(2)), c55a, c13) : c11;
+  const Q4<T> C33 = KIND == VI_MEDIUM_ISO ? C11 : c33;
+  if (surf) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ezz.v[k] = -(C13.v[k] * exx.v[k]) / C33.v[k];
+  }
+  const Q4<T> c55r{{c55a.v[1], c55a.v[2], c55a.v[3], c55a4}}, c55br{{c55b.v[1], c55b.v[2], c55b.v[3], c55b4}};
+  const Q4<T> C55h = mul4(splat4<T>(T(0.25)), add4(add4(add4(c55a, c55r), c55b), c55br));
+  sxx = fma4(dt4, fma4(C11, exx, mul4(C13, ezz)), sxx);
+  szz = fma4(dt4, fma4(C13, exx, mul4(C33, ezz)), szz);
+  sxz = fma4(dt4, mul4(C55h, exz), sxz);
   if constexpr (NSLS > 0) {
 #pragma unroll
     for (int n = 0; n < NSLS; ++n) {
-      const T a1 = a.a1[n], a2 = a.a2[n];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        m[0 * NSLS + n].v[k] += dt * (a1 * rxx[k] + a2 * m[0 * NSLS + n].v[k]);
-        m[1 * NSLS + n].v[k] =
-            surf ? T(0) : m[1 * NSLS + n].v[k] + dt * (a1 * rzz[k] + a2 * m[1 * NSLS + n].v[k]);
-        m[2 * NSLS + n].v[k] += dt * (a1 * rxz[k] + a2 * m[2 * NSLS + n].v[k]);
-      }
+      const Q4<T> a1 = splat4<T>(a.a1[n]), a2 = splat4<T>(a.a2[n]);
+      m[0 * NSLS + n] = fma4(dt4, fma4(a1, rxx, mul4(a2, m[0 * NSLS + n])), m[0 * NSLS + n]);
+      m[1 * NSLS + n] = surf ? splat4<T>(0) : fma4(dt4, fma4(a1, rzz, mul4(a2, m[1 * NSLS + n])), m[1 * NSLS + n]);
+      m[2 * NSLS + n] = fma4(dt4, fma4(a1, rxz, mul4(a2, m[2 * NSLS + n])), m[2 * NSLS + n]);
     }
 #pragma unroll
     for (int q = 0; q < 3 * NSLS; ++q) stg4(a.m + q * a.mstride + g, m[q]);

@@ -99,4 +99,59 @@ __device__ __forceinline__ T dms(const T (&u)[12], int c, const T *D) {  // ddxm
          D[3] * (u[c + 3] - u[c - 4]);
 }
 
+// ---- arithmetic on a 4-cell group.  FP32 pairs of cells use the packed
+// FP32x2 instructions of sm_100 (each lane rounds as the scalar operation
+// does); FP64 stays scalar.
+__device__ __forceinline__ float2 lo2(const Q4<float> &a) { return make_float2(a.v[0], a.v[1]); }
+__device__ __forceinline__ float2 hi2(const Q4<float> &a) { return make_float2(a.v[2], a.v[3]); }
+__device__ __forceinline__ Q4<float> join2(float2 l, float2 h) { return {{l.x, l.y, h.x, h.y}}; }
+template <typename T>
+__device__ __forceinline__ Q4<T> splat4(T s) {
+  return {{s, s, s, s}};
+}
+// a * b + c
+__device__ __forceinline__ Q4<float> fma4(const Q4<float> &a, const Q4<float> &b, const Q4<float> &c) {
+  return join2(__ffma2_rn(lo2(a), lo2(b), lo2(c)), __ffma2_rn(hi2(a), hi2(b), hi2(c)));
+}
+__device__ __forceinline__ Q4<double> fma4(const Q4<double> &a, const Q4<double> &b, const Q4<double> &c) {
+  return {{fma(a.v[0], b.v[0], c.v[0]), fma(a.v[1], b.v[1], c.v[1]), fma(a.v[2], b.v[2], c.v[2]),
+           fma(a.v[3], b.v[3], c.v[3])}};
+}
+__device__ __forceinline__ Q4<float> mul4(const Q4<float> &a, const Q4<float> &b) {
+  return join2(__fmul2_rn(lo2(a), lo2(b)), __fmul2_rn(hi2(a), hi2(b)));
+}
+__device__ __forceinline__ Q4<double> mul4(const Q4<double> &a, const Q4<double> &b) {
+  return {{a.v[0] * b.v[0], a.v[1] * b.v[1], a.v[2] * b.v[2], a.v[3] * b.v[3]}};
+}
+__device__ __forceinline__ Q4<float> add4(const Q4<float> &a, const Q4<float> &b) {
+  return join2(__fadd2_rn(lo2(a), lo2(b)), __fadd2_rn(hi2(a), hi2(b)));
+}
+__device__ __forceinline__ Q4<double> add4(const Q4<double> &a, const Q4<double> &b) {
+  return {{a.v[0] + b.v[0], a.v[1] + b.v[1], a.v[2] + b.v[2], a.v[3] + b.v[3]}};
+}
+template <typename T>
+__device__ __forceinline__ Q4<T> sub4(const Q4<T> &a, const Q4<T> &b) {  // a - b, exact as one rounding
+  return fma4(b, splat4<T>(T(-1)), a);
+}
+// window of 4 consecutive values of a 12-value row, starting at o
+template <typename T>
+__device__ __forceinline__ Q4<T> win4(const T (&u)[12], int o) {
+  return {{u[o], u[o + 1], u[o + 2], u[o + 3]}};
+}
+// the ddxp / ddxm sums of dps / dms for the group's four cells (c = 4..7)
+template <typename T>
+__device__ __forceinline__ Q4<T> dps4(const T (&u)[12], const T *D) {
+  Q4<T> acc = mul4(splat4<T>(D[0]), sub4(win4(u, 5), win4(u, 4)));
+#pragma unroll
+  for (int q = 1; q < 4; ++q) acc = fma4(splat4<T>(D[q]), sub4(win4(u, 5 + q), win4(u, 4 - q)), acc);
+  return acc;
+}
+template <typename T>
+__device__ __forceinline__ Q4<T> dms4(const T (&u)[12], const T *D) {
+  Q4<T> acc = mul4(splat4<T>(D[0]), sub4(win4(u, 4), win4(u, 3)));
+#pragma unroll
+  for (int q = 1; q < 4; ++q) acc = fma4(splat4<T>(D[q]), sub4(win4(u, 4 + q), win4(u, 3 - q)), acc);
+  return acc;
+}
+
 }  // namespace vb
