@@ -73,55 +73,61 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 4 : 2)
       hxz[4 * q + k] = w.v[k];
     }
   }
-  T zxz[4] = {0, 0, 0, 0}, zzz[4] = {0, 0, 0, 0};
+  Q4<T> zxz = splat4<T>(0), zzz = splat4<T>(0);
 #pragma unroll
   for (int q = -4; q <= 4; ++q) {
     if (q <= 3) {  // ddzm(sxz)
       const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
-      const Q4<T> v = q == 0 ? Q4<T>{{hxz[4], hxz[5], hxz[6], hxz[7]}} : ldg4(a.sxz + g + (long long)q * nx);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) zxz[k] += cq * v.v[k];
+      const Q4<T> v = q == 0 ? win4(hxz, 4) : ldg4(a.sxz + g + (long long)q * nx);
+      zxz = fma4(splat4<T>(cq), v, zxz);
     }
     if (q >= -3) {  // ddzp(szz)
       const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
       const Q4<T> v = ldg4(a.szz + g + (long long)q * nx);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) zzz[k] += cq * v.v[k];
+      zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
-  Q4<T> vxn = vxi, vzn = vzi;
+  Q4<T> dxx = dps4(hxx, a.Dx), dxxz = dms4(hxz, a.Dx);
+  if (xstrip) {  // CPML, cell by cell
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int gi = gi0 + k;
-    T dxx = dps(hxx, 4 + k, a.Dx), dxxz = dms(hxz, 4 + k, a.Dx);
-    T dzxz = zxz[k], dzz = zzz[k];
-    if (xstrip) {
+    for (int k = 0; k < 4; ++k) {
+      const int gi = gi0 + k;
       const int xs = strip_x(gi, nx, a.Lx, a.Rx);
       if (xs >= 0) {
         const T *tb = a.tx;
         const long long o = (long long)gj * a.wx + xs;
         T *p0 = a.psix + PX_SXX * a.psix_plane + o, *p1 = a.psix + PX_SXZ * a.psix_plane + o;
-        *p0 = tb[T_BH * nx + gi] * *p0 + tb[T_AH * nx + gi] * dxx;
-        *p1 = tb[T_B * nx + gi] * *p1 + tb[T_A * nx + gi] * dxxz;
-        dxx = dxx * tb[T_IKH * nx + gi] + *p0;
-        dxxz = dxxz * tb[T_IK * nx + gi] + *p1;
+        *p0 = tb[T_BH * nx + gi] * *p0 + tb[T_AH * nx + gi] * dxx.v[k];
+        *p1 = tb[T_B * nx + gi] * *p1 + tb[T_A * nx + gi] * dxxz.v[k];
+        dxx.v[k] = dxx.v[k] * tb[T_IKH * nx + gi] + *p0;
+        dxxz.v[k] = dxxz.v[k] * tb[T_IK * nx + gi] + *p1;
       }
     }
-    if (zs >= 0) {
-      const T *tb = a.tz;
-      const long long o = (long long)zs * nx + gi;
-      T *p0 = a.psiz + PZ_SXZ * a.psiz_plane + o, *p1 = a.psiz + PZ_SZZ * a.psiz_plane + o;
-      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * dzxz;
-      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * dzz;
-      dzxz = dzxz * tb[T_IK * nz + gj] + *p0;
-      dzz = dzz * tb[T_IKH * nz + gj] + *p1;
-    }
-    const T rx = k < 3 ? r0.v[k + 1] : r4;
-    vxn.v[k] = vxi.v[k] + a.dt * two_over_s(r0.v[k] + rx) * (dxx + dzxz);
-    vzn.v[k] = vzi.v[k] + a.dt * two_over_s(r0.v[k] + r1.v[k]) * (dxxz + dzz);
   }
+  if (zs >= 0) {
+    const T *tb = a.tz;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long o = (long long)zs * nx + gi0 + k;
+      T *p0 = a.psiz + PZ_SXZ * a.psiz_plane + o, *p1 = a.psiz + PZ_SZZ * a.psiz_plane + o;
+      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * zxz.v[k];
+      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * zzz.v[k];
+      zxz.v[k] = zxz.v[k] * tb[T_IK * nz + gj] + *p0;
+      zzz.v[k] = zzz.v[k] * tb[T_IKH * nz + gj] + *p1;
+    }
+  }
+  const Q4<T> sx = add4(r0, Q4<T>{{r0.v[1], r0.v[2], r0.v[3], r4}}), sz = add4(r0, r1);
+  Q4<T> bx, bz;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    bx.v[k] = two_over_s(sx.v[k]);
+    bz.v[k] = two_over_s(sz.v[k]);
+  }
+  const Q4<T> dt4 = splat4<T>(a.dt);
+  Q4<T> vxn = fma4(mul4(dt4, bx), add4(dxx, zxz), vxi);
+  Q4<T> vzn = fma4(mul4(dt4, bz), add4(dxxz, zzz), vzi);
   const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
   for (int e = e0; e < e1; ++e) {  // force sources of this tile
     const int4 en = x.tile_ent[e];
