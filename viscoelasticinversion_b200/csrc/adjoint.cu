@@ -516,18 +516,27 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   StepArgs<T> probe = a;
   bind(probe, mk(seg));
   const bool use_split = split_eligible<T>(p, probe);
-  FusedExtras<T> fx{};
+  using SS = SplitStressGeom<T>;
+  FusedExtras<T> fx{}, fxs{};
   SplitMaps ms{};
-  int ntiles = 0;
+  int ntiles = 0, sntiles = 0;
   if (use_split) {
-    int ntx = 0, ntz = 0;
-    std::vector<int> off;
-    std::vector<int4> ent;
+    // velocity tiling and stress tiling, one buffer of lists
+    int ntx = 0, ntz = 0, sntx = 0, sntz = 0;
+    std::vector<int> off, soff;
+    std::vector<int4> ent, sent;
     build_tile_lists(c.nx, c.nz, SG::TX, SG::TZ, 0, shot, off, ent, ntx, ntz);
+    build_tile_lists(c.nx, c.nz, SS::TX, SS::TZ, 0, shot, soff, sent, sntx, sntz);
+    const int nvoff = (int)off.size();
+    for (int v : soff) off.push_back(v + (int)ent.size());
+    ent.insert(ent.end(), sent.begin(), sent.end());
     int *d_off = nullptr;
     int4 *d_ent = nullptr;
     if ((rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent))) return rc;
     ntiles = ntx * ntz;
+    sntiles = sntx * sntz;
+    fxs.ntx = sntx;
+    fxs.tile_off = d_off + nvoff;
     fx.ntx = ntx;
     fx.fs = c.free_surface;
     fx.tile_off = d_off;
@@ -538,6 +547,11 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     fx.nrec = nrec;
     fx.tnt = nt;
     fx.err = (int *)p->errflag;
+    const int sntx_keep = fxs.ntx;
+    const int *soff_keep = fxs.tile_off;
+    fxs = fx;
+    fxs.ntx = sntx_keep;
+    fxs.tile_off = soff_keep;
   }
   auto fwd_step = [&](const Slot<T> &sl, int it, T *traces, bool pdl) -> int {
     if (!use_split) {
@@ -548,12 +562,12 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     }
     StepArgs<T> b = a;
     bind(b, sl);
-    fx.it = it;
-    fx.traces = traces;
-    int r2 = encode_map(&ms.a, b.vx, (int)sizeof(T), c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1);
-    if (!r2) r2 = encode_map(&ms.b, b.vz, (int)sizeof(T), c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1);
+    fx.it = fxs.it = it;
+    fx.traces = fxs.traces = traces;
+    int r2 = encode_map(&ms.a, b.vx, (int)sizeof(T), c.nx, c.nz, 1, 0, SS::BW, SS::BH, 1);
+    if (!r2) r2 = encode_map(&ms.b, b.vz, (int)sizeof(T), c.nx, c.nz, 1, 0, SS::BW, SS::BH, 1);
     if (!r2) r2 = launch_split_vel<T>(b, fx, ntiles, st, pdl);
-    if (!r2) r2 = launch_split_stress<T>(c.medium, b, fx, ms, ntiles, st, true);
+    if (!r2) r2 = launch_split_stress<T>(c.medium, b, fxs, ms, sntiles, st, true);
     return r2;
   };
   // ---- forward sweep with checkpoints and traces ----

@@ -155,9 +155,9 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 4 : 2)
 
 // ------------------------------------------------------------------ stress
 template <typename T, int KIND, int NSLS>
-__global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
-  using G = SplitGeom<T>;
+  using G = SplitStressGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, SW = G::BW, PB = G::PB;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
@@ -337,18 +337,18 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 2 : 1)
 template <typename T, int KIND, int NSLS>
 static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                          int ntiles, cudaStream_t st, bool pdl) {
-  using G = SplitGeom<T>;
+  using SG = SplitStressGeom<T>;
   static unsigned long long attr_set = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
     cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_STRESS);
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS>, dim3(ntiles), dim3(G::NT),
-                               (size_t)G::SMEM_STRESS, st, pdl, a, x, m),
+  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS>, dim3(ntiles), dim3(SG::NT),
+                               (size_t)SG::SMEM, st, pdl, a, x, m),
                     "split stress launch");
 }
 
@@ -399,7 +399,7 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   if (nsteps == 0) return VI_OK;
   // per-tile source/receiver lists of the velocity tiling and (pipelined:
   // its own 64 x 8 tiling) the stress tiling, in one buffer
-  int vtx = G::TX, vtz = G::TZ, stx = G::TX, stz = G::TZ;
+  int vtx = G::TX, vtz = G::TZ, stx = SplitStressGeom<T>::TX, stz = SplitStressGeom<T>::TZ;
   if (pipelined) split_p_tiles(vtx, vtz, stx, stz);
   int ntx, ntz, sntx, sntz;
   std::vector<int> off, soff;
@@ -419,8 +419,9 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   if (pipelined) {
     if ((rc = encode_split_p<T>(c, a, pv, ps))) return rc;
   } else {
-    if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
-    if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, G::BW, G::BH, 1))) return rc;
+    using SG = SplitStressGeom<T>;
+    if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1))) return rc;
+    if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1))) return rc;
     ms.c = ms.b;
   }
   FusedExtras<T> x;

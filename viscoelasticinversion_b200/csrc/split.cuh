@@ -22,6 +22,20 @@ struct SplitGeom {
   static constexpr int SMEM_STRESS = 128 + 2 * PB * (int)sizeof(T);
 };
 
+// Tiling of the stress kernel: 64 x STRESS_TZ cells, one 4-cell group per
+// thread, the new velocities staged as a TMA box with a 4-cell halo.
+constexpr int kStressTZ = 8;
+template <typename T>
+struct SplitStressGeom {
+  static constexpr int TX = 64, TZ = kStressTZ, NT = TX / 4 * TZ;
+  static constexpr int BW = TX + 8, BH = TZ + 8;
+  static constexpr int PB =
+      (int)(((long long)BW * BH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
+  static constexpr int O0 = 128 / (int)sizeof(T);
+  static constexpr int BOX_BYTES = BW * BH * (int)sizeof(T);
+  static constexpr int SMEM = 128 + 2 * PB * (int)sizeof(T);
+};
+
 // TMA maps of the staged planes: (sxx, szz, sxz) for the velocity kernel,
 // (vx, vz) for the stress kernel.
 struct SplitMaps {
