@@ -47,7 +47,7 @@ namespace vb {
 // barrier, so a CTA's loads are all in flight at once and many CTAs fit
 // on an SM.
 template <typename T>
-__global__ void __launch_bounds__(SplitGeom<T>::NT, sizeof(T) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
     k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
   using G = SplitGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ;

@@ -13,7 +13,7 @@ namespace vb {
 
 template <typename T>
 struct SplitGeom {
-  static constexpr int TX = 64, TZ = 16, NT = 256;  // one 4-cell group per thread
+  static constexpr int TX = 64, TZ = 8, NT = TX / 4 * TZ;  // one 4-cell group per thread
   static constexpr int BW = TX + 8, BH = TZ + 8;    // staged box: tile + 4-cell halo
   static constexpr int PB =
       (int)(((long long)BW * BH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
