@@ -87,6 +87,14 @@ template <typename T, int W>
 struct VW {
   T v[W];
 };
+// adds d to lane k (known only at run time) without indexing the register
+// array dynamically (which would move it to the stack)
+template <typename T, int W>
+__device__ __forceinline__ void add_lanew(VW<T, W> &q, int k, T d) {
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    if (i == k) q.v[i] += d;
+}
 template <typename T, int W>
 __device__ __forceinline__ VW<T, W> ldw(const T *p) {
   VW<T, W> o;
@@ -580,8 +588,8 @@ __device__ __forceinline__ void compute_tile(const StepArgs<T> &a, const FusedEx
       const int4 en = x.tile_ent[e];
       if (en.w != TL_EXPLOSIVE || en.y != gj || en.x < gi0 || en.x >= gi0 + W) continue;
       const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
-      sxx.v[en.x - gi0] += dt * x.amp[en.z] * w;
-      szz.v[en.x - gi0] += dt * x.amp[en.z] * w;
+      add_lanew(sxx, en.x - gi0, dt * x.amp[en.z] * w);
+      add_lanew(szz, en.x - gi0, dt * x.amp[en.z] * w);
     }
     if (surf) {
 #pragma unroll

@@ -137,9 +137,9 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
     const T f = x.amp[en.z] * w;
     if (en.w == TL_FORCE_X)
-      vxn.v[k] += a.dt * two_over_s(r0.v[k] + (k < 3 ? r0.v[k + 1] : r4)) * f;
+      add_lane4(vxn, k, a.dt * two_over_s(lane4(r0, k) + (k < 3 ? lane4(r0, k + 1) : r4)) * f);
     else
-      vzn.v[k] += a.dt * two_over_s(r0.v[k] + r1.v[k]) * f;
+      add_lane4(vzn, k, a.dt * two_over_s(lane4(r0, k) + lane4(r1, k)) * f);
   }
   stg4(a.vx + g, vxn);
   stg4(a.vz + g, vzn);
@@ -147,8 +147,8 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
     for (int e = e0; e < e1; ++e) {
       const int4 en = x.tile_ent[e];
       if (en.w != TL_RECEIVER || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
-      x.traces[(long long)en.z * x.tnt + x.it] = vxn.v[en.x - gi0];
-      x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = vzn.v[en.x - gi0];
+      x.traces[(long long)en.z * x.tnt + x.it] = lane4(vxn, en.x - gi0);
+      x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = lane4(vzn, en.x - gi0);
     }
   }
 }
@@ -308,8 +308,8 @@ __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 
     const int4 en = x.tile_ent[e];
     if (en.w != TL_EXPLOSIVE || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
-    sxx.v[en.x - gi0] += dt * x.amp[en.z] * w;
-    szz.v[en.x - gi0] += dt * x.amp[en.z] * w;
+    add_lane4(sxx, en.x - gi0, dt * x.amp[en.z] * w);
+    add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
   }
   if (surf) szz = Q4<T>{{0, 0, 0, 0}};
   stg4(a.sxx + g, sxx);

@@ -293,9 +293,9 @@ __global__ void __launch_bounds__(kNT, 3)
             const float w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : 0.f;
             const float f = x.amp[en.z] * w;
             if (en.w == TL_FORCE_X)
-              vxn.v[k] += dt * two_over_fast(r0.v[k] + (k < 3 ? r0.v[k + 1] : r4)) * f;
+              add_lane4(vxn, k, dt * two_over_fast(lane4(r0, k) + (k < 3 ? lane4(r0, k + 1) : r4)) * f);
             else
-              vzn.v[k] += dt * two_over_fast(r0.v[k] + r1.v[k]) * f;
+              add_lane4(vzn, k, dt * two_over_fast(lane4(r0, k) + lane4(r1, k)) * f);
           }
           if (own) {
             const long long gg = (long long)gj * nx + gi0;
@@ -305,8 +305,8 @@ __global__ void __launch_bounds__(kNT, 3)
               for (int e = e0; e < e1; ++e) {
                 const int4 en = x.chunk_ent[e];
                 if (en.w != TL_RECEIVER || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
-                x.traces[(long long)en.z * x.tnt + x.it] = vxn.v[en.x - gi0];
-                x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = vzn.v[en.x - gi0];
+                x.traces[(long long)en.z * x.tnt + x.it] = lane4(vxn, en.x - gi0);
+                x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = lane4(vzn, en.x - gi0);
               }
             }
           }
@@ -474,8 +474,8 @@ __global__ void __launch_bounds__(kNT, 3)
             const int4 en = x.chunk_ent[e];
             if (en.w != TL_EXPLOSIVE || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
             const float w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : 0.f;
-            sxx.v[en.x - gi0] += dt * x.amp[en.z] * w;
-            szz.v[en.x - gi0] += dt * x.amp[en.z] * w;
+            add_lane4(sxx, en.x - gi0, dt * x.amp[en.z] * w);
+            add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
           }
           if (surf) szz = Q4<float>{{0, 0, 0, 0}};
           stg4(a.sxx_o + gg, sxx);

@@ -42,6 +42,18 @@ __device__ __forceinline__ Q4<double> ldc4(const double *p) {
   const double2 b = reinterpret_cast<const double2 *>(p)[1];
   return {{a.x, a.y, b.x, b.y}};
 }
+// lane k (0..3, known only at run time) of a 4-cell group, without
+// indexing the register array dynamically (which would move it to the stack)
+template <typename T>
+__device__ __forceinline__ T lane4(const Q4<T> &q, int k) {
+  return k == 0 ? q.v[0] : k == 1 ? q.v[1] : k == 2 ? q.v[2] : q.v[3];
+}
+template <typename T>
+__device__ __forceinline__ void add_lane4(Q4<T> &q, int k, T d) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (i == k) q.v[i] += d;
+}
 __device__ __forceinline__ void stg4(float *p, const Q4<float> &q) {
   *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
 }
@@ -62,6 +74,13 @@ template <typename T>
 struct Q2 {
   T v[2];
 };
+template <typename T>
+__device__ __forceinline__ void add_lane2(Q2<T> &q, int k, T d) {
+  if (k == 0)
+    q.v[0] += d;
+  else
+    q.v[1] += d;
+}
 __device__ __forceinline__ Q2<float> lds2(const float *p) {
   const float2 q = *reinterpret_cast<const float2 *>(p);
   return {{q.x, q.y}};
