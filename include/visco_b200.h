@@ -165,13 +165,14 @@ int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
  * with _vel_1Q! (:3-20), _stress_1Q! (:59-85), the free-surface kernels
  * (free-surface-kernels.jl:16-213) and the CPML/ψ recursion
  * (sciml_solver/CPML.jl:291-328).  `shot` may be NULL (no sources or
- * receivers).  kernel_variant: 0 = default (for ISO/VTI with nx % 4 == 0
- * and 16-byte aligned planes the split pair, else the TMA-staged
- * fused kernel when eligible, else the fused kernel), 1 = plain
+ * receivers).  kernel_variant: 0 = default (with nx % 4 == 0 and 16-byte
+ * aligned planes the split pair, else the fused kernel), 1 = plain
  * multi-kernel path (in place), 2 = fused kernel without TMA, 3 = TMA-staged
  * fused kernel (persistent, two stages when they fit), 4 = TMA-staged fused
- * kernel with one stage, 5 = split velocity/stress kernel pair (in place,
- * one tile per CTA), 6 = the split pair as persistent TMA-pipelined kernels,
+ * kernel with one stage, 5 = split velocity/stress kernel pair (one tile
+ * per CTA; in place, TTI with memory variables and CPML psi ping-ponging
+ * through the plan), 6 = the ISO/VTI split pair as persistent
+ * TMA-pipelined kernels,
  * 7 = streaming kernel (FP32 ISO/VTI: persistent CTAs march down 128-column
  * strips with TMA row rings, one launch per step).
  * Variants 3-7 return VI_ERR_ARG when not eligible. */

@@ -49,13 +49,13 @@ def test_parity_with_oracle(oracle_lib, name, precision, variant):
     assert np.abs(tr_ref).max() > 0
     from viscoelasticinversion_b200 import ViError
 
-    if variant in (3, 4, 5, 6) and w.nx % 4 or variant in (5, 6) and w.kind == "tti":
+    if variant in (3, 4, 5, 6) and w.nx % 4 or variant == 6 and w.kind == "tti":
         # not eligible: the explicit variant refuses, the default falls back
         with pytest.raises(ViError):
             run_gpu(w, precision, variant)
         info = {}
         run_gpu(w, precision, 0, nt=4, info=info)
-        assert info["kernel"] == ("fused" if w.nx % 4 else "fused-tma")
+        assert info["kernel"] == ("fused" if w.nx % 4 else "split")
         return
     if variant == 4 and precision == "f64":
         variant_kernel = "fused-tma-1stage"
@@ -73,17 +73,20 @@ def test_parity_with_oracle(oracle_lib, name, precision, variant):
 @pytest.mark.parametrize("kind", ["iso", "vti", "tti"])
 @pytest.mark.parametrize("nsls", [0, 1, 5])
 def test_tma_kernel_mechanism_counts(oracle_lib, kind, nsls):
-    """Every (medium, N_sls) instantiation of the TMA-staged kernel against
-    the oracle (FP32), including the shapes that fall back to 8-row tiles."""
+    """Every (medium, N_sls) instantiation of the default kernels (the split
+    pair) and of the TMA-staged fused kernel against the oracle, including
+    the shapes that fall back to 8-row tiles."""
     w = media.layered(nx=192, nz=100, nt=200, kind=kind, seed=11, pml=12, nrec=16, nsls=nsls)
     tr_ref, st_ref = oracle_lib.run(w, precision="f64")
-    info = {}
-    tr, st = run_gpu(w, "f32", 0, info=info)
-    err = compare(tr, st, tr_ref, st_ref, w.nsls)
-    assert max(err.values()) < 1e-5, (info, err)
-    trd, std = run_gpu(w, "f64", 0, info=info)
-    errd = compare(trd, std, tr_ref, st_ref, w.nsls)
-    assert max(errd.values()) < 1e-10, (info, errd)
+    for variant, name in ((0, "split"), (3, "fused-tma")):
+        info = {}
+        tr, st = run_gpu(w, "f32", variant, info=info)
+        assert info["kernel"] == name
+        err = compare(tr, st, tr_ref, st_ref, w.nsls)
+        assert max(err.values()) < 1e-5, (info, err)
+        trd, std = run_gpu(w, "f64", variant, info=info)
+        errd = compare(trd, std, tr_ref, st_ref, w.nsls)
+        assert max(errd.values()) < 1e-10, (info, errd)
 
 
 @pytest.mark.parametrize("kind", ["iso", "vti", "tti"])
@@ -92,7 +95,7 @@ def test_no_free_surface_with_top_cpml_and_force_sources(oracle_lib, kind):
     w.sources = [(80, 60, 1, 1.0), (81, 59, 2, -0.5), (40, 30, 0, 2.0), (80, 60, 2, 0.25)]
     w.wavelets = np.stack([w.wavelets[0]] * 4)
     tr_ref, st_ref = oracle_lib.run(w, precision="f64")
-    for variant in (1, 2, 3, 4) + ((5, 6) if kind != "tti" else ()):
+    for variant in (1, 2, 3, 4, 5) + ((6,) if kind != "tti" else ()):
         tr, st = run_gpu(w, "f64", variant)
         err = compare(tr, st, tr_ref, st_ref, w.nsls)
         assert max(err.values()) < 1e-10, (variant, err)
@@ -123,6 +126,25 @@ def test_split_chunked_and_mixed_with_fused():
     assert np.array_equal(tr1, tr2)
     tr3, _ = run_gpu(w, "f32", 3, chunks=[150, 150])
     assert rel_l2(tr3, tr1) < 1e-5
+
+
+def test_tti_split_chunked_and_mixed_with_fused():
+    """The TTI split pair ping-pongs M and psi every step: odd and even
+    chunks (M copied back after an odd one) give the same bits as one call,
+    and it shares the plan state with the fused kernel across calls."""
+    w = media.layered(nx=200, nz=140, nt=300, kind="tti", seed=3, pml=16, nrec=24)
+    info = {}
+    tr1, st1 = run_gpu(w, "f32", 5, info=info)
+    assert info["kernel"] == "split"
+    tr2, st2 = run_gpu(w, "f32", 5, chunks=[101, 99, 1, 99])
+    assert np.array_equal(tr1, tr2)
+    for k in st1:
+        assert np.array_equal(st1[k], st2[k]), k
+    tr3, _ = run_gpu(w, "f32", 3, chunks=[150, 150])
+    assert rel_l2(tr3, tr1) < 1e-5
+    tr4, _ = run_gpu(w, "f32", 5, chunks=[77, 1])
+    tr5, _ = run_gpu(w, "f32", 3, chunks=[77, 1])
+    assert rel_l2(tr4[:, :, :78], tr5[:, :, :78]) < 1e-5
 
 
 def test_deterministic():

@@ -1,14 +1,16 @@
-// split.cu — the step as two in-place kernels per time step (ISO and VTI).
+// split.cu — the step as two kernels per time step.
 //
-//   k_split_vel_ldg: v += dt*b*(div sigma + f) on a 64 x 16 tile; every
+//   k_split_vel_ldg: v += dt*b*(div sigma + f) on a 64 x 8 tile; every
 //                    stress tap is an aligned 128-bit load through L1 (the
-//                    tile's loads all in flight at once, no staging).
-//   k_split_stress:  SLS stress + memory variables on a 64 x 16 tile; the
-//                    new velocities of the tile + 4-cell halo are staged by
-//                    TMA, every own-cell operand (sigma, M, stiffness, tau)
-//                    is a 128-bit load issued before the arithmetic.
+//                    tile's loads all in flight at once, no staging).  The
+//                    same kernel serves every medium.
+//   k_split_stress:  ISO/VTI SLS stress + memory variables on a 64 x 8 tile;
+//                    the new velocities of the tile + 4-cell halo are staged
+//                    by TMA, every own-cell operand (sigma, M, stiffness,
+//                    tau) is a 128-bit load issued before the arithmetic.
 //                    Threads on the rows below the free surface also write
 //                    the stress images, so no separate mirror pass is needed.
+//   k_split_stress_tti (split_tti.cu): the TTI stress pass.
 //
 // The kernels of one call are chained by programmatic dependent launch:
 // each is launched while its predecessor drains and waits at entry for it
@@ -21,10 +23,11 @@
 // the stress kernel — 156 B per point per step for FP32 VTI with 3 SLS
 // against 136 B for a single fused pass, but with a fraction of the fused
 // kernel's arithmetic per byte.
-// In place is safe: the velocity kernel reads v only at its own cells and
-// never writes sigma; the stress kernel reads v and writes sigma, M and psi
-// only at its own cells.  (TTI needs neighbours' effective rates and stays
-// on the fused ping-pong kernel.)
+// In place is safe for ISO/VTI: the velocity kernel reads v only at its own
+// cells and never writes sigma; the stress kernel reads v and writes sigma,
+// M and psi only at its own cells.  The TTI stress pass also reads M and
+// psi on a ring of neighbouring cells, so for TTI those two ping-pong
+// between buffers every step (sigma and v stay in place).
 #include <cudaTypedefs.h>
 
 #include <cstdint>
@@ -98,11 +101,12 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
       if (xs >= 0) {
         const T *tb = a.tx;
         const long long o = (long long)gj * a.wx + xs;
-        T *p0 = a.psix + PX_SXX * a.psix_plane + o, *p1 = a.psix + PX_SXZ * a.psix_plane + o;
-        *p0 = tb[T_BH * nx + gi] * *p0 + tb[T_AH * nx + gi] * dxx.v[k];
-        *p1 = tb[T_B * nx + gi] * *p1 + tb[T_A * nx + gi] * dxxz.v[k];
-        dxx.v[k] = dxx.v[k] * tb[T_IKH * nx + gi] + *p0;
-        dxxz.v[k] = dxxz.v[k] * tb[T_IK * nx + gi] + *p1;
+        const T p0 = tb[T_BH * nx + gi] * a.psix[PX_SXX * a.psix_plane + o] + tb[T_AH * nx + gi] * dxx.v[k];
+        const T p1 = tb[T_B * nx + gi] * a.psix[PX_SXZ * a.psix_plane + o] + tb[T_A * nx + gi] * dxxz.v[k];
+        a.psix_o[PX_SXX * a.psix_plane + o] = p0;
+        a.psix_o[PX_SXZ * a.psix_plane + o] = p1;
+        dxx.v[k] = dxx.v[k] * tb[T_IKH * nx + gi] + p0;
+        dxxz.v[k] = dxxz.v[k] * tb[T_IK * nx + gi] + p1;
       }
     }
   }
@@ -111,11 +115,12 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const long long o = (long long)zs * nx + gi0 + k;
-      T *p0 = a.psiz + PZ_SXZ * a.psiz_plane + o, *p1 = a.psiz + PZ_SZZ * a.psiz_plane + o;
-      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * zxz.v[k];
-      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * zzz.v[k];
-      zxz.v[k] = zxz.v[k] * tb[T_IK * nz + gj] + *p0;
-      zzz.v[k] = zzz.v[k] * tb[T_IKH * nz + gj] + *p1;
+      const T p0 = tb[T_B * nz + gj] * a.psiz[PZ_SXZ * a.psiz_plane + o] + tb[T_A * nz + gj] * zxz.v[k];
+      const T p1 = tb[T_BH * nz + gj] * a.psiz[PZ_SZZ * a.psiz_plane + o] + tb[T_AH * nz + gj] * zzz.v[k];
+      a.psiz_o[PZ_SXZ * a.psiz_plane + o] = p0;
+      a.psiz_o[PZ_SZZ * a.psiz_plane + o] = p1;
+      zxz.v[k] = zxz.v[k] * tb[T_IK * nz + gj] + p0;
+      zzz.v[k] = zzz.v[k] * tb[T_IKH * nz + gj] + p1;
     }
   }
   const Q4<T> sx = add4(r0, Q4<T>{{r0.v[1], r0.v[2], r0.v[3], r4}}), sz = add4(r0, r1);
@@ -378,9 +383,10 @@ static bool al16(const void *q) { return ((uintptr_t)q & 15) == 0; }
 template <typename T>
 bool split_eligible(const vi_plan *p, const StepArgs<T> &a) {
   const vi_config &c = p->cfg;
-  if (c.medium == VI_MEDIUM_TTI || c.nx % 4 != 0) return false;
+  if (c.nx % 4 != 0) return false;
   if (((size_t)c.nx * sizeof(T)) % 16 != 0) return false;
-  const void *ptrs[] = {a.vx, a.vz, a.sxx, a.szz, a.sxz, a.rho, a.c11, a.c13, a.c33, a.c55, a.tau, a.m};
+  const void *ptrs[] = {a.vx,  a.vz,  a.sxx, a.szz, a.sxz, a.rho, a.c11,
+                        a.c13, a.c15, a.c33, a.c35, a.c55, a.tau, a.m};
   for (const void *q : ptrs)
     if (q && !al16(q)) return false;
   if (c.nsls > 0 && ((size_t)a.mstride * sizeof(T)) % 16 != 0) return false;
@@ -392,14 +398,36 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
                 bool pipelined) {
   using G = SplitGeom<T>;
   const vi_config &c = p->cfg;
+  const bool tti = c.medium == VI_MEDIUM_TTI;
   if (!split_eligible<T>(p, a))
-    return set_error(VI_ERR_ARG, "split step needs an ISO/VTI medium, nx % 4 == 0 and 16-byte aligned planes");
+    return set_error(VI_ERR_ARG, "split step needs nx % 4 == 0 and 16-byte aligned planes");
+  if (pipelined && tti)
+    return set_error(VI_ERR_ARG, "the pipelined split step covers ISO and VTI media");
   if (pipelined && !split_p_fits(c.medium, c.nsls, (int)sizeof(T)))
     return set_error(VI_ERR_ARG, "pipelined split step does not fit shared memory for this medium");
   if (nsteps == 0) return VI_OK;
+  const size_t np = (size_t)c.nx * c.nz;
+  T *user_m = a.m, *alt_m = nullptr;
+  const long long user_ms = a.mstride;
+  if (tti && c.nsls > 0) {
+    // the plan's second state copy holds the other memory-variable set
+    if (!p->alt) {
+      const size_t bytes = (5 + 3 * (size_t)c.nsls) * np * sizeof(T);
+      size_t have = 0;
+      int rc = ensure_buffer(p, &p->alt, &have, bytes);
+      if (rc) return rc;
+      rc = cuda_check(cudaMemsetAsync(p->alt, 0, bytes, st), "zero alt state");
+      if (rc) return rc;
+    }
+    alt_m = (T *)p->alt + 5 * np;
+  }
   // per-tile source/receiver lists of the velocity tiling and (pipelined:
   // its own 64 x 8 tiling) the stress tiling, in one buffer
   int vtx = G::TX, vtz = G::TZ, stx = SplitStressGeom<T>::TX, stz = SplitStressGeom<T>::TZ;
+  if (tti) {
+    stx = SplitTtiGeom<T>::TX;
+    stz = SplitTtiGeom<T>::TZ;
+  }
   if (pipelined) split_p_tiles(vtx, vtz, stx, stz);
   int ntx, ntz, sntx, sntz;
   std::vector<int> off, soff;
@@ -419,9 +447,10 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   if (pipelined) {
     if ((rc = encode_split_p<T>(c, a, pv, ps))) return rc;
   } else {
-    using SG = SplitStressGeom<T>;
-    if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1))) return rc;
-    if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, SG::BW, SG::BH, 1))) return rc;
+    const int bw = tti ? SplitTtiGeom<T>::BW : SplitStressGeom<T>::BW;
+    const int bh = tti ? SplitTtiGeom<T>::BH : SplitStressGeom<T>::BH;
+    if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
+    if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
     ms.c = ms.b;
   }
   FusedExtras<T> x;
@@ -436,10 +465,20 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   x.tnt = (s && s->nrec) ? s->traces_nt : 0;
   x.nrec = s ? s->nrec : 0;
   x.err = (int *)p->errflag;
-  // in place on the current psi set
-  const int cur = p->psi_cur;
-  if (a.psix) a.psix = a.psix_o = (T *)p->psix + cur * kPsiPerSet * p->psix_plane;
-  if (a.psiz) a.psiz = a.psiz_o = (T *)p->psiz + cur * kPsiPerSet * p->psiz_plane;
+  // ISO/VTI: in place on the current psi set; TTI: from the current set
+  // to the other one, every step
+  T *psix0 = a.psix ? (T *)p->psix : nullptr, *psiz0 = a.psiz ? (T *)p->psiz : nullptr;
+  auto bind_psi = [&](int cur, int out) {
+    if (psix0) {
+      a.psix = psix0 + cur * kPsiPerSet * p->psix_plane;
+      a.psix_o = psix0 + out * kPsiPerSet * p->psix_plane;
+    }
+    if (psiz0) {
+      a.psiz = psiz0 + cur * kPsiPerSet * p->psiz_plane;
+      a.psiz_o = psiz0 + out * kPsiPerSet * p->psiz_plane;
+    }
+  };
+  if (!tti) bind_psi(p->psi_cur, p->psi_cur);
   const int ntiles = ntx * ntz, sntiles = sntx * sntz;
   FusedExtras<T> xs = x;
   xs.ntx = sntx;
@@ -449,11 +488,33 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     if (pipelined) {
       if ((rc = launch_split_vel_p<T>(a, x, pv, ntiles, p->nsm, st))) return rc;
       if ((rc = launch_split_stress_p<T>(c.medium, a, xs, ps, sntiles, p->nsm, st))) return rc;
+    } else if (tti) {
+      const bool from_user = k % 2 == 0;
+      if (alt_m) {
+        a.m = from_user ? user_m : alt_m;
+        a.mstride = from_user ? user_ms : (long long)np;
+        a.m_o = from_user ? alt_m : user_m;
+        a.mstride_o = from_user ? (long long)np : user_ms;
+      }
+      const int cur = p->psi_cur;
+      bind_psi(cur, 1 - cur);
+      if ((rc = launch_split_vel<T>(a, x, ntiles, st, k > 0))) return rc;
+      if ((rc = launch_split_stress_tti<T>(a, xs, ms, sntiles, st, true))) return rc;
+      p->psi_cur = 1 - cur;
     } else {
       // the first kernel of the call starts after everything before it in
       // the stream; the others overlap the tail of their predecessor
       if ((rc = launch_split_vel<T>(a, x, ntiles, st, k > 0))) return rc;
       if ((rc = launch_split_stress<T>(c.medium, a, xs, ms, sntiles, st, true))) return rc;
+    }
+  }
+  if (alt_m && nsteps % 2 == 1) {
+    // the memory variables sit in the plan's copy: bring them back
+    for (int q = 0; q < 3 * c.nsls; ++q) {
+      rc = cuda_check(cudaMemcpyAsync(user_m + q * user_ms, alt_m + q * np, np * sizeof(T),
+                                      cudaMemcpyDeviceToDevice, st),
+                      "copy back memory variables");
+      if (rc) return rc;
     }
   }
   return VI_OK;

@@ -36,6 +36,25 @@ struct SplitStressGeom {
   static constexpr int SMEM = 128 + 2 * PB * (int)sizeof(T);
 };
 
+// Tiling of the TTI stress kernel: 64 x 8 cells; the effective rates are
+// computed on the tile and a one-cell ring (4-aligned: EW x EH), from a TMA
+// box of the new velocities with the ring's 4-cell stencil halo (BW x BH).
+template <typename T>
+struct SplitTtiGeom {
+  static constexpr int TX = 64, TZ = 8, NT = TX / 4 * TZ;
+  static constexpr int BW = TX + 16, BH = TZ + 10;
+  static constexpr int EW = TX + 8, EH = TZ + 2;
+  static constexpr int PB =
+      (int)(((long long)BW * BH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
+  static constexpr int PE =
+      (int)(((long long)EW * EH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
+  static constexpr int O0 = 128 / (int)sizeof(T);
+  static constexpr int BOX_BYTES = BW * BH * (int)sizeof(T);
+  static constexpr int SMEM = 128 + (2 * PB + 3 * PE) * (int)sizeof(T);
+  static constexpr int NRING = 2 * (EW / 4) + 2 * TZ;  // ring groups: 2 rows + 2 columns
+  static_assert(NRING <= NT, "one ring group per thread at most");
+};
+
 // TMA maps of the staged planes: (sxx, szz, sxz) for the velocity kernel,
 // (vx, vz) for the stress kernel.
 struct SplitMaps {
@@ -48,6 +67,12 @@ int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, 
 template <typename T>
 int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
                         const SplitMaps &m, int ntiles, cudaStream_t st, bool pdl);
+// TTI stress pass: reads M (a.m) and psi (a.psix/psiz) of the tile and its
+// ring, writes them to a.m_o and a.psix_o/psiz_o (must differ from the
+// inputs); sigma in place.
+template <typename T>
+int launch_split_stress_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                            int ntiles, cudaStream_t st, bool pdl);
 
 // TMA maps of the pipelined split kernels: velocity (sxx, szz, sxz boxes,
 // vx, vz, rho tiles); stress (vx, vz boxes, sxx, szz, sxz tiles, M, then the
