@@ -220,7 +220,7 @@ def measure_batch(a, dev, stream, max_over_ranks, barrier, world):
     b.run()  # tunes the kernel form, captures the graph, runs once
     b.reset()
     form = b.status()
-    variant = 3 if form == "two-stage" else 4
+    variant = {"split": 5, "two-stage": 3, "one-stage": 4}[form]
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

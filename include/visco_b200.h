@@ -209,8 +209,9 @@ int vi_forward_host(vi_plan *plan, const vi_medium *med_host,
 /* Many shots of different grids and step counts advancing together.  The
  * reference solves one problem per call (ViscoelasticProblem.jl:273-309)
  * and has no batch; this is the B200 form of running its time step for a
- * whole shot gather: one launch per time step covers the tiles of every
- * shot still running, and the sequence of launches is one CUDA graph.
+ * whole shot gather: each launch covers the tiles of every shot still
+ * running (one fused launch, or the split velocity and stress launches,
+ * per time step), and the sequence of launches is one CUDA graph.
  * Shots must share the medium kind, precision and nsls, and have nx % 4 == 0. */
 typedef struct vi_batch vi_batch;
 #define VI_BATCH_NO_GRAPH 1  /* launch step by step instead of one CUDA graph */
@@ -228,8 +229,9 @@ int vi_batch_set_shot(vi_batch *batch, int32_t i, const vi_medium *med_dev,
  * shots to rest (fields, memory variables and CPML memory zeroed) before
  * the run proper.  Every run zeroes the CPML memory first. */
 int vi_batch_run(vi_batch *batch, int32_t flags, void *stream);
-/* Synchronizes, reports the kernel form in use (1 two-stage persistent,
- * 0 one-stage) and any device-side wait failure (VI_ERR_TIMEOUT). */
+/* Synchronizes, reports the kernel form in use (2 split velocity/stress
+ * pair, 1 two-stage persistent fused, 0 one-stage fused) and any
+ * device-side wait failure (VI_ERR_TIMEOUT). */
 int vi_batch_status(vi_batch *batch, void *stream, int32_t *kernel_form);
 
 /* ---- misfit gradient (discrete adjoint) ------------------------------ */

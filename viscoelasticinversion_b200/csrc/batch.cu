@@ -9,9 +9,12 @@
 // step-count order so the shots active at step it are a prefix of the
 // order and a launch covers items [0, prefix[active]).
 //
-// The autotuner picks the kernel form (two-stage persistent tiles or
-// one-stage tiles) by timing a few steps of each on the bound shots and
-// caches the choice per (medium, precision, mechanisms, grid set).
+// Kernel forms: the TMA-staged fused step (one launch per time step; two-
+// stage persistent tiles or one-stage tiles) or the split pair (a velocity
+// and a stress launch per time step, in place; TTI memory variables and
+// psi ping-pong by step parity).  The autotuner picks the form by timing a
+// few steps of each on the bound shots and caches the choice per (medium,
+// precision, mechanisms, grid set).
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -21,6 +24,7 @@
 
 #include "fused_tma.cuh"
 #include "plan.cuh"
+#include "split.cuh"
 
 struct vi_batch {
   int n = 0;
@@ -39,15 +43,17 @@ struct vi_batch {
   int *err = nullptr;
   // cached graph of the whole run (valid while nothing is re-bound)
   cudaGraphExec_t graph = nullptr;
-  bool graph_persist = true;
+  int graph_form = -1;
   bool dirty = true;
-  int persist = -1;  // kernel form: -1 untuned, 0 one-stage, 1 two-stage persistent
+  int form = -1;  // kernel form: -1 untuned, 0 one-stage, 1 two-stage persistent, 2 split pair
   std::vector<int> order;
   std::vector<int> prefix;
   int max_nt = 0;
 };
 
 namespace vb {
+
+constexpr int kFormOneStage = 0, kFormTwoStage = 1, kFormSplit = 2;
 
 static std::map<std::string, int> g_tuned;  // kernel form chosen per problem class
 
@@ -64,13 +70,19 @@ static std::string tune_key(const vi_batch *b) {
 
 // Builds every per-shot device structure for one kernel form and uploads it.
 template <typename T>
-static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) {
-  const TmaBoxes bx = tma_boxes(b->kind, b->nsls, (int)sizeof(T), persist);
-  if (!bx.ok) return set_error(VI_ERR_ARG, "batch: the TMA-staged step does not fit this medium");
+static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
+  const bool split = form == kFormSplit;
+  const bool tti = b->kind == VI_MEDIUM_TTI;
+  TmaBoxes bx{};
+  if (!split) {
+    bx = tma_boxes(b->kind, b->nsls, (int)sizeof(T), form == kFormTwoStage);
+    if (!bx.ok) return set_error(VI_ERR_ARG, "batch: the TMA-staged step does not fit this medium");
+  }
   const int n = b->n;
   std::vector<StepArgs<T>> args(2 * n);
   std::vector<FusedExtras<T>> ext(n);
-  std::vector<TmaMaps> maps(2 * n);
+  std::vector<TmaMaps> maps(split ? 0 : 2 * n);
+  std::vector<SplitMaps> smaps(split ? n : 0);
   std::vector<int> ntiles(n);
   int rc;
   for (int i = 0; i < n; ++i) {
@@ -88,7 +100,10 @@ static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) 
     int ntx, ntz;
     std::vector<int> off;
     std::vector<int4> ent;
-    build_tile_lists(c.nx, c.nz, bx.TX, bx.TZ, bx.HV, &b->shot[i], off, ent, ntx, ntz);
+    if (split)
+      build_tile_lists(c.nx, c.nz, SplitGeom<T>::TX, SplitGeom<T>::TZ, 0, &b->shot[i], off, ent, ntx, ntz);
+    else
+      build_tile_lists(c.nx, c.nz, bx.TX, bx.TZ, bx.HV, &b->shot[i], off, ent, ntx, ntz);
     int *d_off = nullptr;
     int4 *d_ent = nullptr;
     if ((rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent))) return rc;
@@ -100,7 +115,32 @@ static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) 
     for (int q = 0; q < 5; ++q) alt_st[q] = alt + q * np;
     T *psix0 = (T *)p->psix, *psiz0 = (T *)p->psiz;
     p->psi_cur = 0;  // a batch run starts from rest: psi is reset below
-    for (int par = 0; par < 2; ++par) {
+    if (split) {
+      if (!split_eligible<T>(p, a))
+        return set_error(VI_ERR_ARG, "batch: the split step needs 16-byte aligned planes");
+      for (int par = 0; par < 2; ++par) {
+        // sigma and v in place; TTI: M and psi from parity par to the other
+        StepArgs<T> s = a;
+        const int pin = tti ? par : 0, pout = tti ? 1 - par : 0;
+        if (tti) {
+          s.m = par == 0 ? a.m : alt + 5 * np;
+          s.mstride = par == 0 ? a.mstride : (long long)np;
+          s.m_o = par == 0 ? alt + 5 * np : a.m;
+          s.mstride_o = par == 0 ? (long long)np : a.mstride;
+        }
+        s.psix = psix0 ? psix0 + pin * kPsiPerSet * p->psix_plane : nullptr;
+        s.psix_o = psix0 ? psix0 + pout * kPsiPerSet * p->psix_plane : nullptr;
+        s.psiz = psiz0 ? psiz0 + pin * kPsiPerSet * p->psiz_plane : nullptr;
+        s.psiz_o = psiz0 ? psiz0 + pout * kPsiPerSet * p->psiz_plane : nullptr;
+        args[2 * i + par] = s;
+      }
+      const int bw = tti ? SplitTtiGeom<T>::BW : SplitStressGeom<T>::BW;
+      const int bh = tti ? SplitTtiGeom<T>::BH : SplitStressGeom<T>::BH;
+      if ((rc = encode_map(&smaps[i].a, a.vx, (int)sizeof(T), c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
+      if ((rc = encode_map(&smaps[i].b, a.vz, (int)sizeof(T), c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
+      smaps[i].c = smaps[i].b;
+    }
+    for (int par = 0; par < (split ? 0 : 2); ++par) {
       StepArgs<T> s = a;
       T *const *in = par == 0 ? user : alt_st;
       T *const *out = par == 0 ? alt_st : user;
@@ -140,11 +180,12 @@ static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) 
   b->prefix.assign(n + 1, 0);
   for (int q = 0; q < n; ++q) b->prefix[q + 1] = b->prefix[q] + ntiles[b->order[q]];
   b->max_nt = n ? b->nt[b->order[0]] : 0;
-  // one device block: args | ext | maps | prefix | order
+  // one device block: args | ext | maps | smaps | prefix | order
   auto up = [](size_t x) { return (x + 127) / 128 * 128; };
   const size_t o_args = 0, o_ext = up(o_args + args.size() * sizeof(StepArgs<T>));
   const size_t o_maps = up(o_ext + ext.size() * sizeof(FusedExtras<T>));
-  const size_t o_pre = up(o_maps + maps.size() * sizeof(TmaMaps));
+  const size_t o_smaps = up(o_maps + maps.size() * sizeof(TmaMaps));
+  const size_t o_pre = up(o_smaps + smaps.size() * sizeof(SplitMaps));
   const size_t o_ord = up(o_pre + b->prefix.size() * sizeof(int));
   const size_t total = up(o_ord + b->order.size() * sizeof(int));
   if (b->dev_bytes < total) {
@@ -161,6 +202,7 @@ static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) 
   std::memcpy(host.data() + o_args, args.data(), args.size() * sizeof(StepArgs<T>));
   std::memcpy(host.data() + o_ext, ext.data(), ext.size() * sizeof(FusedExtras<T>));
   std::memcpy(host.data() + o_maps, maps.data(), maps.size() * sizeof(TmaMaps));
+  std::memcpy(host.data() + o_smaps, smaps.data(), smaps.size() * sizeof(SplitMaps));
   std::memcpy(host.data() + o_pre, b->prefix.data(), b->prefix.size() * sizeof(int));
   std::memcpy(host.data() + o_ord, b->order.data(), b->order.size() * sizeof(int));
   if ((rc = cuda_check(cudaMemcpyAsync(b->dev, host.data(), total, cudaMemcpyHostToDevice, st),
@@ -171,6 +213,7 @@ static int prepare(vi_batch *b, bool persist, cudaStream_t st, BatchDev<T> &bd) 
   bd.args = (const StepArgs<T> *)(d + o_args);
   bd.ext = (const FusedExtras<T> *)(d + o_ext);
   bd.maps = (const TmaMaps *)(d + o_maps);
+  bd.smaps = (const SplitMaps *)(d + o_smaps);
   bd.prefix = (const int *)(d + o_pre);
   bd.order = (const int *)(d + o_ord);
   bd.nshots = n;
@@ -186,12 +229,20 @@ static int items_at(const vi_batch *b, int it) {
 }
 
 template <typename T>
-static int launch_steps(vi_batch *b, const BatchDev<T> &bd, bool persist, int it0, int it1,
+static int launch_steps(vi_batch *b, const BatchDev<T> &bd, int form, int it0, int it1,
                         cudaStream_t st) {
   for (int it = it0; it < it1; ++it) {
     const int nitems = items_at(b, it);
     if (nitems == 0) break;
-    int rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, it, nitems, b->nsm, persist, st);
+    int rc;
+    if (form == kFormSplit) {
+      // each launch overlaps the tail of the previous one and waits for it
+      // at entry (programmatic dependent launch), as the one-shot pair does
+      rc = launch_split_vel_batch<T>(b->kind, bd, it, nitems, st, it > it0);
+      if (!rc) rc = launch_split_stress_batch<T>(b->kind, b->nsls, bd, it, nitems, st, true);
+    } else {
+      rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, it, nitems, b->nsm, form == kFormTwoStage, st);
+    }
     if (rc) return rc;
   }
   return cuda_check(cudaGetLastError(), "batch launch");
@@ -222,25 +273,27 @@ static int tune(vi_batch *b, cudaStream_t st) {
   const std::string key = tune_key(b);
   auto hit = g_tuned.find(key);
   if (hit != g_tuned.end()) {
-    b->persist = hit->second;
+    b->form = hit->second;
     return VI_OK;
   }
   float best = 1e30f;
-  int choice = 1;
-  const int forms = sizeof(T) == 4 ? 2 : 1;  // double precision has one form
-  for (int f = 0; f < forms; ++f) {
-    const bool persist = f == 0;
+  int choice = kFormTwoStage;
+  // double precision has one fused form (two stages do not fit)
+  const int forms[3] = {kFormSplit, kFormTwoStage, kFormOneStage};
+  const int nforms = sizeof(T) == 4 ? 3 : 2;
+  for (int f = 0; f < nforms; ++f) {
+    const int form = forms[f];
     BatchDev<T> bd;
-    int rc = prepare<T>(b, persist, st, bd);
+    int rc = prepare<T>(b, form, st, bd);
     if (rc == VI_ERR_ARG) continue;
     if (rc) return rc;
     const int steps = std::min(8, b->max_nt);
-    if ((rc = launch_steps<T>(b, bd, persist, 0, 2, st))) return rc;  // warm-up
+    if ((rc = launch_steps<T>(b, bd, form, 0, 2, st))) return rc;  // warm-up
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
-    rc = launch_steps<T>(b, bd, persist, 0, steps, st);
+    rc = launch_steps<T>(b, bd, form, 0, steps, st);
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -250,13 +303,20 @@ static int tune(vi_batch *b, cudaStream_t st) {
     if (rc) return rc;
     if (ms < best) {
       best = ms;
-      choice = persist ? 1 : 0;
+      choice = form;
     }
   }
-  b->persist = choice;
+  b->form = choice;
   g_tuned[key] = choice;
   // tuning advanced the shots: put them back at rest
   return reset_state<T>(b, st);
+}
+
+// Sets kernel attributes (outside a capture) for a form.
+template <typename T>
+static int set_up_form(vi_batch *b, const BatchDev<T> &bd, int form, cudaStream_t st) {
+  if (form == kFormSplit) return launch_split_stress_batch<T>(b->kind, b->nsls, bd, 0, 0, st, false);
+  return launch_fused_tma_batch<T>(b->kind, b->nsls, bd, 0, 0, b->nsm, form == kFormTwoStage, st);
 }
 
 template <typename T>
@@ -266,31 +326,30 @@ static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
   int rc = cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
   if (rc) return rc;
   const bool use_graph = (flags & VI_BATCH_NO_GRAPH) == 0;
-  if (b->persist < 0 || (flags & VI_BATCH_RETUNE)) {
+  if (b->form < 0 || (flags & VI_BATCH_RETUNE)) {
     if (flags & VI_BATCH_RETUNE) g_tuned.erase(tune_key(b));
     if ((rc = tune<T>(b, st))) return rc;
     b->dirty = true;
   }
-  const bool persist = b->persist == 1;
+  const int form = b->form;
   for (int i = 0; i < b->n; ++i)
     if ((rc = vi_plan_reset(b->plans[i], st))) return rc;
-  if (b->dirty || !use_graph || b->graph_persist != persist) {
+  if (b->dirty || !use_graph || b->graph_form != form) {
     BatchDev<T> bd;
-    if ((rc = prepare<T>(b, persist, st, bd))) return rc;
+    if ((rc = prepare<T>(b, form, st, bd))) return rc;
     if (b->graph) {
       cudaGraphExecDestroy(b->graph);
       b->graph = nullptr;
     }
     if (use_graph) {
-      // kernel attributes are set outside the capture
-      if ((rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, 0, 0, b->nsm, persist, st))) return rc;
+      if ((rc = set_up_form<T>(b, bd, form, st))) return rc;
       cudaStream_t cs;
       if ((rc = cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream")))
         return rc;
       cudaGraph_t g = nullptr;
       rc = cuda_check(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
       if (!rc) {
-        const int lrc = launch_steps<T>(b, bd, persist, 0, b->max_nt, cs);
+        const int lrc = launch_steps<T>(b, bd, form, 0, b->max_nt, cs);
         rc = cuda_check(cudaStreamEndCapture(cs, &g), "end capture");
         if (!rc) rc = lrc;
       }
@@ -298,25 +357,30 @@ static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
       if (g) cudaGraphDestroy(g);
       cudaStreamDestroy(cs);
       if (rc) return rc;
-      b->graph_persist = persist;
+      b->graph_form = form;
       b->dirty = false;
     } else {
-      if ((rc = launch_steps<T>(b, bd, persist, 0, b->max_nt, st))) return rc;
+      if ((rc = launch_steps<T>(b, bd, form, 0, b->max_nt, st))) return rc;
     }
   }
   if (use_graph && (rc = cuda_check(cudaGraphLaunch(b->graph, st), "graph launch"))) return rc;
   // shots with an odd step count end in the plan's copy: bring them back
+  // (the fused forms ping-pong the whole state, the split pair only the
+  // TTI memory variables)
   for (int i = 0; i < b->n; ++i) {
     if (b->nt[i] % 2 == 0) continue;
+    if (form == kFormSplit && b->kind != VI_MEDIUM_TTI) continue;
     vi_plan *p = b->plans[i];
     const size_t np = (size_t)p->cfg.nx * p->cfg.nz;
     T *alt = (T *)p->alt;
     const vi_fields &f = b->fields[i];
-    void *user[5] = {f.vx, f.vz, f.sxx, f.szz, f.sxz};
-    for (int q = 0; q < 5; ++q)
-      if ((rc = cuda_check(cudaMemcpyAsync(user[q], alt + q * np, np * sizeof(T), cudaMemcpyDeviceToDevice, st),
-                           "copy back fields")))
-        return rc;
+    if (form != kFormSplit) {
+      void *user[5] = {f.vx, f.vz, f.sxx, f.szz, f.sxz};
+      for (int q = 0; q < 5; ++q)
+        if ((rc = cuda_check(cudaMemcpyAsync(user[q], alt + q * np, np * sizeof(T), cudaMemcpyDeviceToDevice, st),
+                             "copy back fields")))
+          return rc;
+    }
     for (int q = 0; q < 3 * p->cfg.nsls; ++q)
       if ((rc = cuda_check(cudaMemcpyAsync((T *)f.m + q * f.m_plane_stride, alt + (5 + q) * np,
                                            np * sizeof(T), cudaMemcpyDeviceToDevice, st),
@@ -420,7 +484,7 @@ extern "C" int vi_batch_status(vi_batch *b, void *stream, int32_t *kernel_form) 
   if (!b) return set_error(VI_ERR_ARG, "batch is NULL");
   int rc = cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "batch status");
   if (rc) return rc;
-  if (kernel_form) *kernel_form = b->persist;
+  if (kernel_form) *kernel_form = b->form;
   int flag = 0;
   rc = cuda_check(cudaMemcpy(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
   if (rc) return rc;

@@ -101,17 +101,39 @@ template <typename T>
 int launch_fused_tma(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
                      const TmaMaps &maps, int ntiles, int nsm, bool persist, cudaStream_t st);
 
-// Per-shot data of a batch in device memory (see k_fused_tma_batch).
+struct SplitMaps;
+
+// Per-shot data of a batch in device memory (see k_fused_tma_batch and the
+// batched split kernels).
 template <typename T>
 struct BatchDev {
   const StepArgs<T> *args;    // [2 * nshots]: index 2*s + parity of the step
   const FusedExtras<T> *ext;  // [nshots] (it is set per launch)
-  const TmaMaps *maps;        // [2 * nshots]
+  const TmaMaps *maps;        // [2 * nshots] (fused kernel forms)
+  const SplitMaps *smaps;     // [nshots] (split kernel form)
   const int *prefix;          // [nshots + 1] tile offsets in processing order
   const int *order;           // [nshots] shot at each processing position
   int nshots;
   int *err;
 };
+
+#ifdef __CUDACC__
+// The shot and tile of batch item `item` (items are the tiles of the shots
+// in processing order): the largest position p with prefix[p] <= item.
+template <typename T>
+__device__ __forceinline__ void batch_locate(const BatchDev<T> &b, int item, int &shot, int &tile) {
+  int lo = 0, hi = b.nshots - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.prefix[mid] <= item)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  shot = b.order[lo];
+  tile = item - b.prefix[lo];
+}
+#endif
 
 template <typename T>
 int launch_fused_tma_batch(int kind, int nsls, const BatchDev<T> &b, int it, int nitems, int nsm,

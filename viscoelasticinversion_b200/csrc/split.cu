@@ -49,13 +49,14 @@ namespace vb {
 // windows start on multiples of 4), no shared-memory staging and no
 // barrier, so a CTA's loads are all in flight at once and many CTAs fit
 // on an SM.
-template <typename T>
-__global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
-    k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
+// PP: psi read from the input set and written to the output set (TTI);
+// else in place on the input set.
+template <typename T, bool PP>
+__device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
+                                               int tile) {
   using G = SplitGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ;
-  pdl_wait();  // the previous stress pass is complete and visible
-  const int tile = blockIdx.x;
+  T *const psix_o = PP ? a.psix_o : a.psix, *const psiz_o = PP ? a.psiz_o : a.psiz;
   const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
   const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
   const int tid = threadIdx.x;
@@ -103,8 +104,8 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
         const long long o = (long long)gj * a.wx + xs;
         const T p0 = tb[T_BH * nx + gi] * a.psix[PX_SXX * a.psix_plane + o] + tb[T_AH * nx + gi] * dxx.v[k];
         const T p1 = tb[T_B * nx + gi] * a.psix[PX_SXZ * a.psix_plane + o] + tb[T_A * nx + gi] * dxxz.v[k];
-        a.psix_o[PX_SXX * a.psix_plane + o] = p0;
-        a.psix_o[PX_SXZ * a.psix_plane + o] = p1;
+        psix_o[PX_SXX * a.psix_plane + o] = p0;
+        psix_o[PX_SXZ * a.psix_plane + o] = p1;
         dxx.v[k] = dxx.v[k] * tb[T_IKH * nx + gi] + p0;
         dxxz.v[k] = dxxz.v[k] * tb[T_IK * nx + gi] + p1;
       }
@@ -117,8 +118,8 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
       const long long o = (long long)zs * nx + gi0 + k;
       const T p0 = tb[T_B * nz + gj] * a.psiz[PZ_SXZ * a.psiz_plane + o] + tb[T_A * nz + gj] * zxz.v[k];
       const T p1 = tb[T_BH * nz + gj] * a.psiz[PZ_SZZ * a.psiz_plane + o] + tb[T_AH * nz + gj] * zzz.v[k];
-      a.psiz_o[PZ_SXZ * a.psiz_plane + o] = p0;
-      a.psiz_o[PZ_SZZ * a.psiz_plane + o] = p1;
+      psiz_o[PZ_SXZ * a.psiz_plane + o] = p0;
+      psiz_o[PZ_SZZ * a.psiz_plane + o] = p1;
       zxz.v[k] = zxz.v[k] * tb[T_IK * nz + gj] + p0;
       zzz.v[k] = zzz.v[k] * tb[T_IKH * nz + gj] + p1;
     }
@@ -158,17 +159,36 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
   }
 }
 
+template <typename T, bool PP>
+__global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
+    k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
+  pdl_wait();  // the previous stress pass is complete and visible
+  split_vel_tile<T, PP>(a, x, blockIdx.x);
+}
+
+// Batched: one tile of one shot per CTA; the step parity selects the shot's
+// argument set (ping-pong buffers for TTI).
+template <typename T, bool PP>
+__global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
+    k_split_vel_batch(const BatchDev<T> b, int it) {
+  pdl_wait();
+  int shot, tile;
+  batch_locate(b, blockIdx.x, shot, tile);
+  FusedExtras<T> x = b.ext[shot];
+  x.it = it;
+  split_vel_tile<T, PP>(b.args[2 * shot + (it & 1)], x, tile);
+}
+
 // ------------------------------------------------------------------ stress
 template <typename T, int KIND, int NSLS>
-__global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
-    k_split_stress(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
+__device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
+                                                  const SplitMaps &maps, int tile) {
   using G = SplitStressGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, SW = G::BW, PB = G::PB;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
   T *s_vx = reinterpret_cast<T *>(smem_raw) + G::O0;
   T *s_vz = s_vx + PB;
-  const int tile = blockIdx.x;
   const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
   const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
   const int tid = threadIdx.x;
@@ -338,6 +358,23 @@ __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 
   }
 }
 
+template <typename T, int KIND, int NSLS>
+__global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
+    k_split_stress(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
+                   const __grid_constant__ SplitMaps maps) {
+  split_stress_tile<T, KIND, NSLS>(a, x, maps, blockIdx.x);
+}
+
+template <typename T, int KIND, int NSLS>
+__global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
+    k_split_stress_batch(const BatchDev<T> b, int it) {
+  int shot, tile;
+  batch_locate(b, blockIdx.x, shot, tile);
+  FusedExtras<T> x = b.ext[shot];
+  x.it = it;
+  split_stress_tile<T, KIND, NSLS>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+}
+
 // ------------------------------------------------------------------- host
 template <typename T, int KIND, int NSLS>
 static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
@@ -361,8 +398,11 @@ template <typename T>
 int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, cudaStream_t st,
                      bool pdl) {
   using G = SplitGeom<T>;
-  return cuda_check(launch_pdl(k_split_vel_ldg<T>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x),
-                    "split velocity launch");
+  const bool pp = a.psix_o != a.psix || a.psiz_o != a.psiz;
+  const cudaError_t e =
+      pp ? launch_pdl(k_split_vel_ldg<T, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+         : launch_pdl(k_split_vel_ldg<T, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
+  return cuda_check(e, "split velocity launch");
 }
 
 template <typename T>
@@ -376,6 +416,50 @@ int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
 #undef VB_KIND
 #undef VB_CASE
   return set_error(VI_ERR_ARG, "the split step covers ISO and VTI media");
+}
+
+template <typename T>
+int launch_split_vel_batch(int kind, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
+                           bool pdl) {
+  using G = SplitGeom<T>;
+  if (nitems <= 0) return VI_OK;
+  const cudaError_t e =
+      kind == VI_MEDIUM_TTI
+          ? launch_pdl(k_split_vel_batch<T, true>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it)
+          : launch_pdl(k_split_vel_batch<T, false>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it);
+  return cuda_check(e, "batched split velocity launch");
+}
+
+template <typename T, int KIND, int NSLS>
+static int launch_stress_batch(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+  using SG = SplitStressGeom<T>;
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set & (1ULL << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_batch<T, KIND, NSLS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
+    if (e != cudaSuccess) return cuda_check(e, "batched split stress smem attribute");
+    attr_set |= 1ULL << dev;
+  }
+  if (nitems <= 0) return VI_OK;  // attribute set-up only
+  return cuda_check(launch_pdl(k_split_stress_batch<T, KIND, NSLS>, dim3(nitems), dim3(SG::NT),
+                               (size_t)SG::SMEM, st, pdl, b, it),
+                    "batched split stress launch");
+}
+
+template <typename T>
+int launch_split_stress_batch(int kind, int nsls, const BatchDev<T> &b, int it, int nitems,
+                              cudaStream_t st, bool pdl) {
+  if (kind == VI_MEDIUM_TTI) return launch_split_stress_tti_batch<T>(nsls, b, it, nitems, st, pdl);
+#define VB_CASE(K, N) \
+  if (kind == K && nsls == N) return launch_stress_batch<T, K, N>(b, it, nitems, st, pdl);
+#define VB_KIND(K) VB_CASE(K, 0) VB_CASE(K, 1) VB_CASE(K, 2) VB_CASE(K, 3) VB_CASE(K, 4) VB_CASE(K, 5)
+  VB_KIND(VI_MEDIUM_ISO)
+  VB_KIND(VI_MEDIUM_VTI)
+#undef VB_KIND
+#undef VB_CASE
+  return set_error(VI_ERR_ARG, "batched split step: unknown medium or nsls");
 }
 
 static bool al16(const void *q) { return ((uintptr_t)q & 15) == 0; }
@@ -527,6 +611,13 @@ template int split_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int
 template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int,
                                  cudaStream_t, bool);
 
+template int launch_split_vel_batch<float>(int, const BatchDev<float> &, int, int, cudaStream_t, bool);
+template int launch_split_vel_batch<double>(int, const BatchDev<double> &, int, int, cudaStream_t,
+                                            bool);
+template int launch_split_stress_batch<float>(int, int, const BatchDev<float> &, int, int,
+                                              cudaStream_t, bool);
+template int launch_split_stress_batch<double>(int, int, const BatchDev<double> &, int, int,
+                                               cudaStream_t, bool);
 template int launch_split_vel<float>(const StepArgs<float> &, const FusedExtras<float> &, int,
                                      cudaStream_t, bool);
 template int launch_split_vel<double>(const StepArgs<double> &, const FusedExtras<double> &, int,

@@ -6,6 +6,7 @@
 
 #include "common.cuh"
 #include "fused.cuh"
+#include "fused_tma.cuh"
 
 struct vi_plan;
 
@@ -67,6 +68,18 @@ int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, 
 template <typename T>
 int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
                         const SplitMaps &m, int ntiles, cudaStream_t st, bool pdl);
+// The split pair over the tiles of many shots (BatchDev, per-shot v-box
+// maps in smaps): item i of a launch is the tile batch_locate gives.
+template <typename T>
+int launch_split_vel_batch(int kind, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
+                           bool pdl);
+template <typename T>
+int launch_split_stress_batch(int kind, int nsls, const BatchDev<T> &b, int it, int nitems,
+                              cudaStream_t st, bool pdl);
+template <typename T>
+int launch_split_stress_tti_batch(int nsls, const BatchDev<T> &b, int it, int nitems,
+                                  cudaStream_t st, bool pdl);
+
 // TTI stress pass: reads M (a.m) and psi (a.psix/psiz) of the tile and its
 // ring, writes them to a.m_o and a.psix_o/psiz_o (must differ from the
 // inputs); sigma in place.

@@ -133,8 +133,8 @@ __device__ __forceinline__ Q4<T> mean4_fwd(const Q4<T> &a, T a4, const Q4<T> &b,
 }
 
 template <typename T, int NSLS>
-__global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
-    k_split_stress_tti(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
+__device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
+                                                      const SplitMaps &maps, int tile) {
   using G = SplitTtiGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, BW = G::BW, EW = G::EW, EG = G::EW / 4;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -142,7 +142,6 @@ __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 2
   T *s_vx = reinterpret_cast<T *>(smem_raw) + G::O0;
   T *s_vz = s_vx + G::PB;
   T *s_exx = s_vz + G::PB, *s_ezz = s_exx + G::PE, *s_exz = s_ezz + G::PE;
-  const int tile = blockIdx.x;
   const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
   const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
   const int tid = threadIdx.x;
@@ -286,6 +285,25 @@ __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 2
 }
 
 template <typename T, int NSLS>
+__global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
+    k_split_stress_tti(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
+                       const __grid_constant__ SplitMaps maps) {
+  split_stress_tti_tile<T, NSLS>(a, x, maps, blockIdx.x);
+}
+
+// Batched: one tile of one shot per CTA; the step parity selects the
+// shot's M / psi buffers.
+template <typename T, int NSLS>
+__global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
+    k_split_stress_tti_batch(const BatchDev<T> b, int it) {
+  int shot, tile;
+  batch_locate(b, blockIdx.x, shot, tile);
+  FusedExtras<T> x = b.ext[shot];
+  x.it = it;
+  split_stress_tti_tile<T, NSLS>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+}
+
+template <typename T, int NSLS>
 static int launch_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
                       cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
@@ -317,6 +335,42 @@ int launch_split_stress_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const
   }
 }
 
+template <typename T, int NSLS>
+static int launch_tti_batch(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+  using G = SplitTtiGeom<T>;
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set & (1ULL << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti_batch<T, NSLS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    if (e != cudaSuccess) return cuda_check(e, "batched split TTI stress smem attribute");
+    attr_set |= 1ULL << dev;
+  }
+  if (nitems <= 0) return VI_OK;  // attribute set-up only
+  return cuda_check(launch_pdl(k_split_stress_tti_batch<T, NSLS>, dim3(nitems), dim3(G::NT),
+                               (size_t)G::SMEM, st, pdl, b, it),
+                    "batched split TTI stress launch");
+}
+
+template <typename T>
+int launch_split_stress_tti_batch(int nsls, const BatchDev<T> &b, int it, int nitems,
+                                  cudaStream_t st, bool pdl) {
+  switch (nsls) {
+    case 0: return launch_tti_batch<T, 0>(b, it, nitems, st, pdl);
+    case 1: return launch_tti_batch<T, 1>(b, it, nitems, st, pdl);
+    case 2: return launch_tti_batch<T, 2>(b, it, nitems, st, pdl);
+    case 3: return launch_tti_batch<T, 3>(b, it, nitems, st, pdl);
+    case 4: return launch_tti_batch<T, 4>(b, it, nitems, st, pdl);
+    case 5: return launch_tti_batch<T, 5>(b, it, nitems, st, pdl);
+    default: return set_error(VI_ERR_ARG, "nsls must be 0..5");
+  }
+}
+
+template int launch_split_stress_tti_batch<float>(int, const BatchDev<float> &, int, int,
+                                                  cudaStream_t, bool);
+template int launch_split_stress_tti_batch<double>(int, const BatchDev<double> &, int, int,
+                                                   cudaStream_t, bool);
 template int launch_split_stress_tti<float>(const StepArgs<float> &, const FusedExtras<float> &,
                                             const SplitMaps &, int, cudaStream_t, bool);
 template int launch_split_stress_tti<double>(const StepArgs<double> &, const FusedExtras<double> &,
