@@ -123,8 +123,9 @@ def measured_peaks():
 
 KERNEL_NAMES = {"fused-tma": "k_fused_tma", "fused-tma-1stage": "k_fused_tma", "fused": "k_fused",
                 "plain": "k_plain", "split": "k_split", "split-pipelined": "k_split_p",
-                "stream": "k_stream"}
-KERNEL_PAIRS = {"split": "k_split_vel + k_split_stress",
+                "split-ldg": "k_split", "stream": "k_stream"}
+KERNEL_PAIRS = {"split": "k_split_vel_tma + k_split_stress",
+                "split-ldg": "k_split_vel_ldg + k_split_stress",
                 "split-pipelined": "k_split_vel_p + k_split_stress_p"}
 
 

@@ -152,7 +152,8 @@ int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
 int vi_plan_status(vi_plan *plan, void *stream);
 /* Which kernel the last vi_step ran: 1 plain, 2 fused, 3 fused TMA-staged,
  * 4 fused TMA-staged single-stage, 5 split velocity/stress pair, 6 split
- * pair, persistent and TMA-pipelined, 7 streaming. */
+ * pair, persistent and TMA-pipelined, 7 streaming, 8 split pair with the
+ * direct-load velocity pass. */
 int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
 
 /* ---- time stepping ------------------------------------------------------ */
@@ -174,8 +175,10 @@ int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
  * through the plan), 6 = the ISO/VTI split pair as persistent
  * TMA-pipelined kernels,
  * 7 = streaming kernel (FP32 ISO/VTI: persistent CTAs march down 128-column
- * strips with TMA row rings, one launch per step).
- * Variants 3-7 return VI_ERR_ARG when not eligible. */
+ * strips with TMA row rings, one launch per step),
+ * 8 = the split pair of 5 with its velocity pass reading the stress taps
+ * straight through L1 instead of TMA boxes.
+ * Variants 3-8 return VI_ERR_ARG when not eligible. */
 int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);

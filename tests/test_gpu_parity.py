@@ -38,18 +38,18 @@ def oracle_run(oracle_lib, name):
     return _cache[name]
 
 
-KERNEL_OF_VARIANT = {1: "plain", 2: "fused", 3: "fused-tma", 4: "fused-tma-1stage", 5: "split", 6: "split-pipelined"}
+KERNEL_OF_VARIANT = {1: "plain", 2: "fused", 3: "fused-tma", 4: "fused-tma-1stage", 5: "split", 6: "split-pipelined", 8: "split-ldg"}
 
 
 @pytest.mark.parametrize("name", ["iso256", "vti256x128", "tti256x128", "iso-odd37x29"])
 @pytest.mark.parametrize("precision", ["f32", "f64"])
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 8])
 def test_parity_with_oracle(oracle_lib, name, precision, variant):
     w, tr_ref, st_ref = oracle_run(oracle_lib, name)
     assert np.abs(tr_ref).max() > 0
     from viscoelasticinversion_b200 import ViError
 
-    if variant in (3, 4, 5, 6) and w.nx % 4 or variant == 6 and w.kind == "tti":
+    if variant in (3, 4, 5, 6, 8) and w.nx % 4 or variant == 6 and w.kind == "tti":
         # not eligible: the explicit variant refuses, the default falls back
         with pytest.raises(ViError):
             run_gpu(w, precision, variant)
@@ -145,6 +145,23 @@ def test_tti_split_chunked_and_mixed_with_fused():
     tr4, _ = run_gpu(w, "f32", 5, chunks=[77, 1])
     tr5, _ = run_gpu(w, "f32", 3, chunks=[77, 1])
     assert rel_l2(tr4[:, :, :78], tr5[:, :, :78]) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["iso", "vti", "tti"])
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_velocity_pass_forms_bit_identical(kind, precision):
+    """The TMA-staged velocity pass (default) and the direct-load one
+    (variant 8, also used by the batch and the gradient sweeps) compute the
+    same bits."""
+    w = media.layered(nx=256, nz=136, nt=160, kind=kind, seed=3, pml=16, nrec=24)
+    info = {}
+    a = run_gpu(w, precision, 5, info=info)
+    assert info["kernel"] == "split"
+    b = run_gpu(w, precision, 8, info=info)
+    assert info["kernel"] == "split-ldg"
+    assert np.array_equal(a[0], b[0])
+    for k in a[1]:
+        assert np.array_equal(a[1][k], b[1][k]), k
 
 
 def test_deterministic():

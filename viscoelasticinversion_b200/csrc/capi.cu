@@ -281,7 +281,7 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   rc = check_fields(p, f);
   if (rc) return rc;
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
-  if (variant < 0 || variant > 7) return set_error(VI_ERR_ARG, "unknown kernel variant");
+  if (variant < 0 || variant > 8) return set_error(VI_ERR_ARG, "unknown kernel variant");
   if (s && s->nrec > 0 && s->traces_nt > 0 && !s->traces_dev)
     return set_error(VI_ERR_ARG, "receivers need traces_dev");
   rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
@@ -327,13 +327,13 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     } else {
       return set_error(VI_ERR_ARG, "the streaming step is FP32 only");
     }
-  } else if (variant == 5 || variant == 6 || (variant == 0 && split_eligible<T>(p, a))) {
+  } else if (variant == 5 || variant == 6 || variant == 8 || (variant == 0 && split_eligible<T>(p, a))) {
     // the one-tile-per-CTA pair measures faster than the pipelined pair on
     // B200 (2048 x 1024 VTI: 27.6 vs 24.4 Gpt/s), so it is the default
-    const bool pipe = variant == 6;
-    rc = split_steps<T>(p, a, s, it0, nsteps, st, pipe);
+    const int mode = variant == 6 ? kSplitPipelined : variant == 8 ? kSplitLdg : kSplitVelTma;
+    rc = split_steps<T>(p, a, s, it0, nsteps, st, mode);
     if (rc) return rc;
-    p->last_kernel = pipe ? 6 : 5;
+    p->last_kernel = variant == 0 ? 5 : variant;
   } else {
     rc = fused_steps<T>(p, a, s, it0, nsteps, st, variant);
     if (rc) return rc;

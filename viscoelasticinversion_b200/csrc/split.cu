@@ -1,9 +1,11 @@
 // split.cu — the step as two kernels per time step.
 //
-//   k_split_vel_ldg: v += dt*b*(div sigma + f) on a 64 x 8 tile; every
+//   k_split_vel_tma: v += dt*b*(div sigma + f) on a 64 x 8 tile from TMA
+//                    boxes of the stress taps (the default; below).
+//   k_split_vel_ldg: the same update on a 64 x 8 tile where every
 //                    stress tap is an aligned 128-bit load through L1 (the
-//                    tile's loads all in flight at once, no staging).  The
-//                    same kernel serves every medium.
+//                    tile's loads all in flight at once, no staging).  Both
+//                    velocity kernels serve every medium.
 //   k_split_stress:  ISO/VTI SLS stress + memory variables on a 64 x 8 tile;
 //                    the new velocities of the tile + 4-cell halo are staged
 //                    by TMA, every own-cell operand (sigma, M, stiffness,
@@ -49,48 +51,16 @@ namespace vb {
 // windows start on multiples of 4), no shared-memory staging and no
 // barrier, so a CTA's loads are all in flight at once and many CTAs fit
 // on an SM.
-// PP: psi read from the input set and written to the output set (TTI);
-// else in place on the input set.
+// CPML, buoyancy, update, force sources, stores and receivers of one
+// 4-cell group whose stress derivatives' raw parts are in hxx/hxz (row
+// windows) and zxz/zzz (z derivatives).
 template <typename T, bool PP>
-__device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
-                                               int tile) {
-  using G = SplitGeom<T>;
-  constexpr int TX = G::TX, TZ = G::TZ;
-  T *const psix_o = PP ? a.psix_o : a.psix, *const psiz_o = PP ? a.psiz_o : a.psiz;
-  const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
-  const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
-  const int tid = threadIdx.x;
-  const int r = tid / (TX / 4), lx = 4 * (tid % (TX / 4));
-  const int gi0 = x0 + lx, gj = z0 + r;
-  if (gi0 >= xe || gj >= ze) return;
-  const long long g = (long long)gj * nx + gi0;
-  const Q4<T> vxi = ldc4(a.vx + g), vzi = ldc4(a.vz + g);
-  const Q4<T> r0 = ldg4(a.rho + g), r1 = ldg4(a.rho + g + nx);
-  const T r4 = __ldg(a.rho + g + 4);
-  T hxx[12], hxz[12];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {  // row windows [gi0-4, gi0+8)
-    const Q4<T> u = ldg4(a.sxx + g - 4 + 4 * q), w = ldg4(a.sxz + g - 4 + 4 * q);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      hxx[4 * q + k] = u.v[k];
-      hxz[4 * q + k] = w.v[k];
-    }
-  }
-  Q4<T> zxz = splat4<T>(0), zzz = splat4<T>(0);
-#pragma unroll
-  for (int q = -4; q <= 4; ++q) {
-    if (q <= 3) {  // ddzm(sxz)
-      const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
-      const Q4<T> v = q == 0 ? win4(hxz, 4) : ldg4(a.sxz + g + (long long)q * nx);
-      zxz = fma4(splat4<T>(cq), v, zxz);
-    }
-    if (q >= -3) {  // ddzp(szz)
-      const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
-      const Q4<T> v = ldg4(a.szz + g + (long long)q * nx);
-      zzz = fma4(splat4<T>(cq), v, zzz);
-    }
-  }
+__device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const FusedExtras<T> &x, int tile,
+                                                 int gi0, int gj, long long g, const Q4<T> &vxi,
+                                                 const Q4<T> &vzi, const Q4<T> &r0, const Q4<T> &r1, T r4,
+                                                 const T (&hxx)[12], const T (&hxz)[12], Q4<T> zxz,
+                                                 Q4<T> zzz, T *psix_o, T *psiz_o) {
+  const int nx = a.nx, nz = a.nz;
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
   Q4<T> dxx = dps4(hxx, a.Dx), dxxz = dms4(hxz, a.Dx);
@@ -157,6 +127,146 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
       x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = lane4(vzn, en.x - gi0);
     }
   }
+}
+
+// PP: psi read from the input set and written to the output set (TTI);
+// else in place on the input set.
+template <typename T, bool PP>
+__device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
+                                               int tile) {
+  using G = SplitGeom<T>;
+  constexpr int TX = G::TX, TZ = G::TZ;
+  T *const psix_o = PP ? a.psix_o : a.psix, *const psiz_o = PP ? a.psiz_o : a.psiz;
+  const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * TZ;
+  const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
+  const int tid = threadIdx.x;
+  const int r = tid / (TX / 4), lx = 4 * (tid % (TX / 4));
+  const int gi0 = x0 + lx, gj = z0 + r;
+  if (gi0 >= xe || gj >= ze) return;
+  const long long g = (long long)gj * nx + gi0;
+  const Q4<T> vxi = ldc4(a.vx + g), vzi = ldc4(a.vz + g);
+  const Q4<T> r0 = ldg4(a.rho + g), r1 = ldg4(a.rho + g + nx);
+  const T r4 = __ldg(a.rho + g + 4);
+  T hxx[12], hxz[12];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {  // row windows [gi0-4, gi0+8)
+    const Q4<T> u = ldg4(a.sxx + g - 4 + 4 * q), w = ldg4(a.sxz + g - 4 + 4 * q);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      hxx[4 * q + k] = u.v[k];
+      hxz[4 * q + k] = w.v[k];
+    }
+  }
+  Q4<T> zxz = splat4<T>(0), zzz = splat4<T>(0);
+#pragma unroll
+  for (int q = -4; q <= 4; ++q) {
+    if (q <= 3) {  // ddzm(sxz)
+      const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
+      const Q4<T> v = q == 0 ? win4(hxz, 4) : ldg4(a.sxz + g + (long long)q * nx);
+      zxz = fma4(splat4<T>(cq), v, zxz);
+    }
+    if (q >= -3) {  // ddzp(szz)
+      const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
+      const Q4<T> v = ldg4(a.szz + g + (long long)q * nx);
+      zzz = fma4(splat4<T>(cq), v, zzz);
+    }
+  }
+  split_vel_finish<T, PP>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+}
+
+// Tile height of the TMA-staged velocity pass (64 x 8: 34.8 Gpt/s on the
+// 2048 x 1024 VTI step; 64 x 16: 34.3; 64 x 32: 33.0).
+constexpr int kVelTmaTZ = 8;
+
+// Velocity pass with the stress taps staged by TMA (the default): one
+// elected thread issues the tile's three stress boxes (sxx 72 x 8 from
+// (x0-4, z0); sxz 72 x 16 from (x0-4, z0-4); szz 64 x 16 from (x0, z0-4))
+// on one mbarrier, so all of a tile's DRAM reads are in flight at CTA
+// start without holding registers, and the stencil reads come from shared
+// memory (2048 x 1024 VTI: 34.8 vs 34.2 Gpt/s for the direct-load pass,
+// which the batched step and the gradient's forward sweeps use).
+template <typename T>
+struct SplitVelTma {
+  static constexpr int TX = 64, TZ = kVelTmaTZ, NT = TX / 4 * TZ;
+  static constexpr int WX = TX + 8, WZ = TX;  // box widths of sxx/sxz and szz
+  static constexpr int HZ = TZ + 8;           // rows of the sxz and szz boxes
+  static constexpr int O_SXX = 128 / (int)sizeof(T);
+  static constexpr int O_SXZ = O_SXX + WX * TZ;
+  static constexpr int O_SZZ = O_SXZ + WX * HZ;
+  static constexpr int BYTES_TX = (WX * TZ + WX * HZ + WZ * HZ) * (int)sizeof(T);
+  static constexpr int SMEM = 128 + BYTES_TX;
+  static_assert((WX * TZ * sizeof(T)) % 16 == 0 && (WX * HZ * sizeof(T)) % 16 == 0, "16-byte boxes");
+};
+
+template <typename T, bool PP>
+__device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
+                                                   const SplitMaps &maps, int tile) {
+  using G = SplitVelTma<T>;
+  constexpr int TX = G::TX, WX = G::WX, WZ = G::WZ;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
+  const T *s_sxx = reinterpret_cast<T *>(smem_raw) + G::O_SXX;
+  const T *s_sxz = reinterpret_cast<T *>(smem_raw) + G::O_SXZ;
+  const T *s_szz = reinterpret_cast<T *>(smem_raw) + G::O_SZZ;
+  T *const psix_o = PP ? a.psix_o : a.psix, *const psiz_o = PP ? a.psiz_o : a.psiz;
+  const int x0 = L + (tile % x.ntx) * TX, z0 = L + (tile / x.ntx) * G::TZ;
+  const int nx = a.nx, nz = a.nz, xe = nx - L, ze = nz - L;
+  const int tid = threadIdx.x;
+  if (tid == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(bar, G::BYTES_TX);
+    tma_load_2d(reinterpret_cast<T *>(smem_raw) + G::O_SXX, &maps.a, x0 - 4, z0, bar);
+    tma_load_2d(reinterpret_cast<T *>(smem_raw) + G::O_SXZ, &maps.b, x0 - 4, z0 - 4, bar);
+    tma_load_2d(reinterpret_cast<T *>(smem_raw) + G::O_SZZ, &maps.c, x0, z0 - 4, bar);
+  }
+  const int r = tid / (TX / 4), lx = 4 * (tid % (TX / 4));
+  const int gi0 = x0 + lx, gj = z0 + r;
+  const bool act = gi0 < xe && gj < ze;
+  const long long g = (long long)gj * nx + gi0;
+  Q4<T> vxi{}, vzi{}, r0{}, r1{};
+  T r4 = 0;
+  if (act) {
+    vxi = ldc4(a.vx + g);
+    vzi = ldc4(a.vz + g);
+    r0 = ldg4(a.rho + g);
+    r1 = ldg4(a.rho + g + nx);
+    r4 = __ldg(a.rho + g + 4);
+  }
+  const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicExch(x.err, 1);
+      mbar_wait_bounded(bar, 0, 1u << 22);
+    }
+    return;
+  }
+  if (!act) return;
+  T hxx[12], hxz[12];
+  row12s(s_sxx + r * WX + lx, hxx);
+  row12s(s_sxz + (r + 4) * WX + lx, hxz);
+  Q4<T> zxz = splat4<T>(0), zzz = splat4<T>(0);
+#pragma unroll
+  for (int q = -4; q <= 4; ++q) {
+    if (q <= 3) {  // ddzm(sxz)
+      const T cq = q >= 0 ? a.Dz[q] : -a.Dz[-q - 1];
+      const Q4<T> v = q == 0 ? win4(hxz, 4) : lds4(s_sxz + (r + 4 + q) * WX + lx + 4);
+      zxz = fma4(splat4<T>(cq), v, zxz);
+    }
+    if (q >= -3) {  // ddzp(szz)
+      const T cq = q >= 1 ? a.Dz[q - 1] : -a.Dz[-q];
+      const Q4<T> v = lds4(s_szz + (r + 4 + q) * WZ + lx);
+      zzz = fma4(splat4<T>(cq), v, zzz);
+    }
+  }
+  split_vel_finish<T, PP>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+}
+
+template <typename T, bool PP>
+__global__ void __launch_bounds__(SplitVelTma<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitVelTma<T>::NT)
+    k_split_vel_tma(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
+  pdl_wait();  // the previous stress pass is complete and visible
+  split_vel_tma_tile<T, PP>(a, x, maps, blockIdx.x);
 }
 
 template <typename T, bool PP>
@@ -478,8 +588,30 @@ bool split_eligible(const vi_plan *p, const StepArgs<T> &a) {
 }
 
 template <typename T>
+static int launch_vel_tma(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                          int ntiles, cudaStream_t st, bool pdl) {
+  using G = SplitVelTma<T>;
+  const bool pp = a.psix_o != a.psix || a.psiz_o != a.psiz;
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set & (1ULL << dev))) {
+    for (auto k : {k_split_vel_tma<T, true>, k_split_vel_tma<T, false>}) {
+      const cudaError_t ea = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+      if (ea != cudaSuccess) return cuda_check(ea, "split velocity (TMA) smem attribute");
+    }
+    attr_set |= 1ULL << dev;
+  }
+  const cudaError_t e =
+      pp ? launch_pdl(k_split_vel_tma<T, true>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
+         : launch_pdl(k_split_vel_tma<T, false>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m);
+  return cuda_check(e, "split velocity (TMA) launch");
+}
+
+template <typename T>
 int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st,
-                bool pipelined) {
+                int mode) {
+  const bool pipelined = mode == kSplitPipelined, vel_tma = mode == kSplitVelTma;
   using G = SplitGeom<T>;
   const vi_config &c = p->cfg;
   const bool tti = c.medium == VI_MEDIUM_TTI;
@@ -508,6 +640,10 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   // per-tile source/receiver lists of the velocity tiling and (pipelined:
   // its own 64 x 8 tiling) the stress tiling, in one buffer
   int vtx = G::TX, vtz = G::TZ, stx = SplitStressGeom<T>::TX, stz = SplitStressGeom<T>::TZ;
+  if (vel_tma) {
+    vtx = SplitVelTma<T>::TX;
+    vtz = SplitVelTma<T>::TZ;
+  }
   if (tti) {
     stx = SplitTtiGeom<T>::TX;
     stz = SplitTtiGeom<T>::TZ;
@@ -526,7 +662,7 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   int rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent);
   if (rc) return rc;
   const int e = sizeof(T);
-  SplitMaps ms;
+  SplitMaps ms, mv;
   SplitPMaps pv, ps;
   if (pipelined) {
     if ((rc = encode_split_p<T>(c, a, pv, ps))) return rc;
@@ -536,6 +672,12 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     if ((rc = encode_map(&ms.a, a.vx, e, c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
     if ((rc = encode_map(&ms.b, a.vz, e, c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
     ms.c = ms.b;
+    if (vel_tma) {
+      using VG = SplitVelTma<T>;
+      if ((rc = encode_map(&mv.a, a.sxx, e, c.nx, c.nz, 1, 0, VG::WX, VG::TZ, 1))) return rc;
+      if ((rc = encode_map(&mv.b, a.sxz, e, c.nx, c.nz, 1, 0, VG::WX, VG::HZ, 1))) return rc;
+      if ((rc = encode_map(&mv.c, a.szz, e, c.nx, c.nz, 1, 0, VG::WZ, VG::HZ, 1))) return rc;
+    }
   }
   FusedExtras<T> x;
   x.ntx = ntx;
@@ -582,13 +724,17 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
       }
       const int cur = p->psi_cur;
       bind_psi(cur, 1 - cur);
-      if ((rc = launch_split_vel<T>(a, x, ntiles, st, k > 0))) return rc;
+      if ((rc = vel_tma ? launch_vel_tma<T>(a, x, mv, ntiles, st, k > 0)
+                        : launch_split_vel<T>(a, x, ntiles, st, k > 0)))
+        return rc;
       if ((rc = launch_split_stress_tti<T>(a, xs, ms, sntiles, st, true))) return rc;
       p->psi_cur = 1 - cur;
     } else {
       // the first kernel of the call starts after everything before it in
       // the stream; the others overlap the tail of their predecessor
-      if ((rc = launch_split_vel<T>(a, x, ntiles, st, k > 0))) return rc;
+      if ((rc = vel_tma ? launch_vel_tma<T>(a, x, mv, ntiles, st, k > 0)
+                        : launch_split_vel<T>(a, x, ntiles, st, k > 0)))
+        return rc;
       if ((rc = launch_split_stress<T>(c.medium, a, xs, ms, sntiles, st, true))) return rc;
     }
   }
@@ -607,9 +753,9 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
 template bool split_eligible<float>(const vi_plan *, const StepArgs<float> &);
 template bool split_eligible<double>(const vi_plan *, const StepArgs<double> &);
 template int split_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int, int, cudaStream_t,
-                                bool);
+                                int);
 template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int,
-                                 cudaStream_t, bool);
+                                 cudaStream_t, int);
 
 template int launch_split_vel_batch<float>(int, const BatchDev<float> &, int, int, cudaStream_t, bool);
 template int launch_split_vel_batch<double>(int, const BatchDev<double> &, int, int, cudaStream_t,

@@ -108,9 +108,12 @@ void split_p_tiles(int &vtx, int &vtz, int &stx, int &stz);
 // one-tile-per-CTA kernels or (pipelined) the persistent TMA-pipelined
 // kernels.  Returns VI_ERR_ARG (without side effects) when the
 // configuration is not eligible (TTI, nx % 4 != 0 or unaligned planes).
+// Velocity pass of split_steps: TMA-staged stress taps (default), direct
+// L1 loads, or the persistent TMA-pipelined pair (ISO/VTI).
+enum SplitMode { kSplitVelTma = 0, kSplitLdg = 1, kSplitPipelined = 2 };
 template <typename T>
 int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st,
-                bool pipelined);
+                int mode);
 
 // true when split_steps can run this plan and these pointers
 template <typename T>

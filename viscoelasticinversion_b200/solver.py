@@ -140,7 +140,7 @@ class StepPlan:
         k = C.c_int32()
         check(lib().vi_plan_last_kernel(self._h, C.byref(k)))
         return {0: "none", 1: "plain", 2: "fused", 3: "fused-tma", 4: "fused-tma-1stage",
-                5: "split", 6: "split-pipelined", 7: "stream"}[k.value]
+                5: "split", 6: "split-pipelined", 7: "stream", 8: "split-ldg"}[k.value]
 
     def zeros_state(self) -> dict:
         """Zeroed device state {vx, vz, sxx, szz, sxz, m}."""
