@@ -124,36 +124,66 @@ __device__ __forceinline__ T cpml_fwd(T d, T p0, T a, T b, T ik, T *pn) {
 }
 
 // ---- images^T: fold the ghost-row adjoints into the rows they mirror ----
+// (all eight rows of a column are loaded before any store: the ghost and
+// target rows are distinct, so the read-modify-writes need not serialise)
 template <typename T>
 __global__ void k_mirror_t(T *sb_zz, T *sb_xz, int nx) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nx) return;
+  T gz[L], tz[L], gq[L], tq[L];
 #pragma unroll
   for (int k = 1; k <= L; ++k) {
-    const long long g = (long long)(L - k) * nx + i;
-    sb_zz[(long long)(L + k) * nx + i] -= sb_zz[g];
-    sb_zz[g] = T(0);
+    gz[k - 1] = sb_zz[(long long)(L - k) * nx + i];
+    tz[k - 1] = sb_zz[(long long)(L + k) * nx + i];
   }
 #pragma unroll
   for (int k = 0; k < L; ++k) {
-    const long long g = (long long)(L - 1 - k) * nx + i;
-    sb_xz[(long long)(L + k) * nx + i] -= sb_xz[g];
-    sb_xz[g] = T(0);
+    gq[k] = sb_xz[(long long)(L - 1 - k) * nx + i];
+    tq[k] = sb_xz[(long long)(L + k) * nx + i];
+  }
+#pragma unroll
+  for (int k = 1; k <= L; ++k) {
+    sb_zz[(long long)(L + k) * nx + i] = tz[k - 1] - gz[k - 1];
+    sb_zz[(long long)(L - k) * nx + i] = T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < L; ++k) {
+    sb_xz[(long long)(L + k) * nx + i] = tq[k] - gq[k];
+    sb_xz[(long long)(L - 1 - k) * nx + i] = T(0);
   }
 }
 
 // ---- S^T: SLS stress stage transposed, per cell of the update region ----
-// scratch planes: rbar[0..3] = (xx, zz, zx, xz) strain-rate adjoints, q = dt*sxzbar*exz
-template <typename T>
+// scratch planes: rbar[0..3] = (xx, zz, zx, xz) strain-rate adjoints, q = dt*sxzbar*exz.
+// N (mechanisms) is a template parameter and every operand is loaded
+// before the arithmetic, so the memory-variable and gradient
+// read-modify-writes do not wait on one another.
+template <typename T, int N>
 __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot<T> x1, Slot<T> ab,
                                                    T *rbar, T *q, double *gc11, double *gc13,
                                                    double *gc33, double *gtau) {
+  constexpr int NM = N > 0 ? N : 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
   if (i >= A.nx - L || j >= A.nz - L) return;
   const int nx = A.nx;
   const long long c = (long long)j * nx + i, np = A.np;
-  const int N = A.nsls;
+  // ---- loads
+  T mo[3 * NM], mbo[3 * NM];
+#pragma unroll
+  for (int k = 0; k < 3 * N; ++k) {
+    mo[k] = x0.m()[k * np + c];
+    mbo[k] = ab.m()[k * np + c];
+  }
+  T *sbx = ab.sxx(), *sbz = ab.szz(), *sbq = ab.sxz();
+  const T bxx = sbx[c], bzz = sbz[c], bxz = sbq[c];
+  const double g11o = gc11[c], g13o = gc13[c], g33o = gc33[c];
+  const double gto = N > 0 ? gtau[c] : 0.0;
+  const T tau = N > 0 ? A.tau[c] : T(0);
+  const T c13 = A.c13[c], c55 = A.c55[c];
+  const T c11 = A.kind == VI_MEDIUM_ISO ? T(0) : A.c11[c];
+  const T c33 = A.kind == VI_MEDIUM_ISO ? T(0) : A.c33[c];
+  const T c55r = A.c55[c + 1], c55b = A.c55[c + nx], c55br = A.c55[c + nx + 1];
   // forward strain rates from v(n+1) with the psi of step n
   T r[4];  // xx = ddxm vx, zz = ddzm vz, zx = ddzp vx, xz = ddxp vz
   r[0] = tap_m(x1.vx(), c, 1, A.Dx);
@@ -162,6 +192,7 @@ __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot
   r[3] = tap_p(x1.vz(), c, 1, A.Dx);
   T ik[4] = {1, 1, 1, 1}, ca[4] = {0, 0, 0, 0}, cb[4] = {0, 0, 0, 0};
   T *pb[4] = {nullptr, nullptr, nullptr, nullptr};
+  T pbo[4] = {0, 0, 0, 0};
   const int xs = strip_x(i, nx, A.Lx, A.Rx), zs = strip_z(j, A.nz, A.Tz, A.Bz);
   if (xs >= 0) {
     const long long o = (long long)j * A.wx + xs;
@@ -173,6 +204,8 @@ __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot
     r[3] = cpml_fwd(r[3], x0.psix()[PX_VZ * A.psix_plane + o], ca[3], cb[3], ik[3], &pn);
     pb[0] = ab.psix() + PX_VX * A.psix_plane + o;
     pb[3] = ab.psix() + PX_VZ * A.psix_plane + o;
+    pbo[0] = *pb[0];
+    pbo[3] = *pb[3];
   }
   if (zs >= 0) {
     const int nz = A.nz;
@@ -184,65 +217,75 @@ __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot
     r[2] = cpml_fwd(r[2], x0.psiz()[PZ_VX * A.psiz_plane + o], ca[2], cb[2], ik[2], &pn);
     pb[1] = ab.psiz() + PZ_VZ * A.psiz_plane + o;
     pb[2] = ab.psiz() + PZ_VX * A.psiz_plane + o;
+    pbo[1] = *pb[1];
+    pbo[2] = *pb[2];
   }
+  // ---- arithmetic
   const T rt[3] = {r[0], r[1], r[2] + r[3]};  // xx, zz, engineering xz
   T S[3] = {0, 0, 0};
+#pragma unroll
   for (int n = 0; n < N; ++n)
-    for (int k = 0; k < 3; ++k) S[k] += x0.m()[(k * N + n) * np + c];
-  const T tau = N > 0 ? A.tau[c] : T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S[k] += mo[k * N + n];
   T e[3];
+#pragma unroll
   for (int k = 0; k < 3; ++k) e[k] = N > 0 ? (T(1) + tau) * rt[k] + tau * S[k] : rt[k];
-  const T C13 = A.c13[c];
-  const T C11 = A.kind == VI_MEDIUM_ISO ? C13 + T(2) * A.c55[c] : A.c11[c];
-  const T C33 = A.kind == VI_MEDIUM_ISO ? C11 : A.c33[c];
-  const T C55h = T(0.25) * (A.c55[c] + A.c55[c + 1] + A.c55[c + nx] + A.c55[c + nx + 1]);
+  const T C13 = c13;
+  const T C11 = A.kind == VI_MEDIUM_ISO ? C13 + T(2) * c55 : c11;
+  const T C33 = A.kind == VI_MEDIUM_ISO ? C11 : c33;
+  const T C55h = T(0.25) * (c55 + c55r + c55b + c55br);
   const bool surf = A.fs && j == L;
-  T *sbx = ab.sxx(), *sbz = ab.szz(), *sbq = ab.sxz();
-  const T bxx = sbx[c], bzz = sbz[c], bxz = sbq[c];
   const T dt = A.dt;
   T eb[3];
+  double g11 = g11o, g13 = g13o, g33 = g33o;
   if (!surf) {
     eb[0] = dt * (C11 * bxx + C13 * bzz);
     eb[1] = dt * (C13 * bxx + C33 * bzz);
-    gc11[c] += (double)dt * bxx * e[0];
-    gc13[c] += (double)dt * (bxx * e[1] + bzz * e[0]);
-    gc33[c] += (double)dt * bzz * e[1];
+    g11 += (double)dt * bxx * e[0];
+    g13 += (double)dt * (bxx * e[1] + bzz * e[0]);
+    g33 += (double)dt * bzz * e[1];
   } else {
     // sxx' = sxx + dt (C11 - C13^2/C33) exx; szz' = 0
     const T ceff = C11 - C13 * C13 / C33;
     eb[0] = dt * ceff * bxx;
     eb[1] = T(0);
     const double w = (double)dt * bxx * e[0];
-    gc11[c] += w;
-    gc13[c] += w * (-2.0 * (double)C13 / (double)C33);
-    gc33[c] += w * ((double)C13 * C13 / ((double)C33 * C33));
+    g11 += w;
+    g13 += w * (-2.0 * (double)C13 / (double)C33);
+    g33 += w * ((double)C13 * C13 / ((double)C33 * C33));
     sbz[c] = T(0);
   }
+  gc11[c] = g11;
+  gc13[c] = g13;
+  gc33[c] = g33;
   eb[2] = dt * C55h * bxz;
   q[c] = dt * bxz * e[2];
   if (N > 0) {
     double gt = 0;
+#pragma unroll
     for (int k = 0; k < 3; ++k) gt += (double)eb[k] * ((double)rt[k] + S[k]);
-    gtau[c] += gt;
+    gtau[c] = gto + gt;
   }
   // memory variables and the strain-rate adjoints
   T rtb[3];
+#pragma unroll
   for (int k = 0; k < 3; ++k) rtb[k] = (N > 0 ? (T(1) + tau) : T(1)) * eb[k];
+#pragma unroll
   for (int n = 0; n < N; ++n) {
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
-      T *mb = ab.m() + (k * N + n) * np + c;
       const bool dead = surf && k == 1;  // Mzz' = 0 on the surface
-      const T mbo = dead ? T(0) : *mb;
-      rtb[k] += dt * A.a1[n] * mbo;
-      *mb = tau * eb[k] + mbo * (T(1) + dt * A.a2[n]);
-      if (dead) *mb = T(0);
+      const T mb = dead ? T(0) : mbo[k * N + n];
+      rtb[k] += dt * A.a1[n] * mb;
+      ab.m()[(k * N + n) * np + c] = dead ? T(0) : tau * eb[k] + mb * (T(1) + dt * A.a2[n]);
     }
   }
   // psi transposes: rbar = rtbar/kappa + a (psibar' + rtbar), psibar = b (...)
   T rb[4] = {rtb[0], rtb[1], rtb[2], rtb[2]};
+#pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (pb[k]) {
-      const T P = *pb[k] + rb[k];
+      const T P = pbo[k] + rb[k];
       *pb[k] = cb[k] * P;
       rb[k] = rb[k] * ik[k] + ca[k] * P;
     }
@@ -631,7 +674,14 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     for (int it = s1 - 1; it >= s0; --it) {
       const Slot<T> x0 = mk(seg + (size_t)(it - s0) * slot), x1 = mk(seg + (size_t)(it - s0 + 1) * slot);
       if (c.free_surface) k_mirror_t<T><<<(c.nx + 127) / 128, 128, 0, st>>>(ab.szz(), ab.sxz(), c.nx);
-      k_stress_t<T><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt);
+      switch (N) {
+        case 0: k_stress_t<T, 0><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 1: k_stress_t<T, 1><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 2: k_stress_t<T, 2><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 3: k_stress_t<T, 3><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 4: k_stress_t<T, 4><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        default: k_stress_t<T, 5><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+      }
       k_gather_c55<T><<<gA, blk, 0, st>>>(q, g55, c.nx, c.nz);
       k_rates_t<T><<<gU, blk, 0, st>>>(A, ab, rbar);
       k_residual<T><<<(nrec + 127) / 128, 128, 0, st>>>(ab, x1, (const int2 *)p->drec, nrec, obs, nt, it, c.nx);
