@@ -293,30 +293,19 @@ __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot
   }
 }
 
-// gc55 gathers the 4 half-node terms that average mu around each cell
-template <typename T>
-__global__ void k_gather_c55(const T *q, double *gc55, int nx, int nz) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= nx || j >= nz) return;
-  double s = 0;
-  for (int dj = 0; dj <= 1; ++dj)
-    for (int di = 0; di <= 1; ++di) {
-      const int ii = i - di, jj = j - dj;
-      if (ii >= 0 && jj >= 0) s += q[(long long)jj * nx + ii];
-    }
-  gc55[(long long)j * nx + i] += 0.25 * s;
-}
 
-// v += -D^T rbar over the update region
+// v += -D^T rbar over the update region (its taps reach at most L cells,
+// so they stay inside the planes; rbar is zero outside the region)
 template <typename T>
 __global__ void k_rates_t(AdjArgs<T> A, Slot<T> ab, const T *rbar) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
   if (i >= A.nx - L || j >= A.nz - L) return;
-  const int nx = A.nx, nz = A.nz;
+  const int nx = A.nx;
   const long long c = (long long)j * nx + i, np = A.np;
-  ab.vx()[c] -= tap_p_b(rbar, i, j, nx, nz, 0, A.Dx) + tap_m_b(rbar + 2 * np, i, j, nx, nz, 1, A.Dz);
-  ab.vz()[c] -= tap_p_b(rbar + np, i, j, nx, nz, 1, A.Dz) + tap_m_b(rbar + 3 * np, i, j, nx, nz, 0, A.Dx);
+  const T vx = ab.vx()[c], vz = ab.vz()[c];
+  ab.vx()[c] = vx - (tap_p(rbar, c, 1, A.Dx) + tap_m(rbar + 2 * np, c, nx, A.Dz));
+  ab.vz()[c] = vz - (tap_p(rbar + np, c, nx, A.Dz) + tap_m(rbar + 3 * np, c, 1, A.Dx));
 }
 
 // residual at the receivers of step it: vbar += d - obs
@@ -366,6 +355,9 @@ __global__ void __launch_bounds__(256) k_vel_t(AdjArgs<T> A, Slot<T> x0, Slot<T>
     pb[1] = ab.psiz() + PZ_SXZ * A.psiz_plane + o;
     pb[3] = ab.psiz() + PZ_SZZ * A.psiz_plane + o;
   }
+  T pbo[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) pbo[k] = pb[k] ? *pb[k] : T(0);
   const T bx = T(2) / (A.rho[c] + A.rho[c + 1]);
   const T bz = T(2) / (A.rho[c] + A.rho[c + nx]);
   const T vbx = ab.vx()[c], vbz = ab.vz()[c];
@@ -373,9 +365,10 @@ __global__ void __launch_bounds__(256) k_vel_t(AdjArgs<T> A, Slot<T> x0, Slot<T>
   h[c] = A.dt * T(-0.5) * bx * bx * (d[0] + d[1]) * vbx;
   h[np + c] = A.dt * T(-0.5) * bz * bz * (d[2] + d[3]) * vbz;
   T db[4] = {A.dt * bx * vbx, A.dt * bx * vbx, A.dt * bz * vbz, A.dt * bz * vbz};
+#pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (pb[k]) {
-      const T P = *pb[k] + db[k];
+      const T P = pbo[k] + db[k];
       *pb[k] = cb[k] * P;
       db[k] = db[k] * ik[k] + ca[k] * P;
     }
@@ -402,16 +395,25 @@ __global__ void k_force_rho_t(AdjArgs<T> A, Slot<T> ab, const int4 *src, const T
   }
 }
 
-// grho gathers h of the two velocity nodes each density value feeds
+// grho gathers h of the two velocity nodes each density value feeds;
+// gc55 gathers the 4 half-node terms q that average mu around each cell
 template <typename T>
-__global__ void k_gather_rho(const T *h, double *grho, int nx, int nz) {
+__global__ void k_gather(const T *h, double *grho, const T *q, double *gc55, int nx, int nz) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= nx || j >= nz) return;
   const long long c = (long long)j * nx + i, np = (long long)nx * nz;
+  const double gr = grho[c], g55 = gc55[c];
   double s = (double)h[c] + (double)h[np + c];
   if (i > 0) s += h[c - 1];
   if (j > 0) s += h[np + c - nx];
-  grho[c] += s;
+  double t = 0;
+  for (int dj = 0; dj <= 1; ++dj)
+    for (int di = 0; di <= 1; ++di) {
+      const int ii = i - di, jj = j - dj;
+      if (ii >= 0 && jj >= 0) t += q[(long long)jj * nx + ii];
+    }
+  grho[c] = gr + s;
+  gc55[c] = g55 + 0.25 * t;
 }
 
 // sigma += -D^T dbar over every cell the velocity stencil reads (ghost rows
@@ -422,9 +424,16 @@ __global__ void k_div_t(AdjArgs<T> A, Slot<T> ab, const T *dbar) {
   if (i >= A.nx || j >= A.nz) return;
   const int nx = A.nx, nz = A.nz;
   const long long c = (long long)j * nx + i, np = A.np;
-  ab.sxx()[c] -= tap_m_b(dbar, i, j, nx, nz, 0, A.Dx);
-  ab.sxz()[c] -= tap_p_b(dbar + np, i, j, nx, nz, 1, A.Dz) + tap_p_b(dbar + 2 * np, i, j, nx, nz, 0, A.Dx);
-  ab.szz()[c] -= tap_m_b(dbar + 3 * np, i, j, nx, nz, 1, A.Dz);
+  const T sxx = ab.sxx()[c], sxz = ab.sxz()[c], szz = ab.szz()[c];
+  if (i >= L && i < nx - L && j >= L && j < nz - L) {  // taps inside the planes: unchecked
+    ab.sxx()[c] = sxx - tap_m(dbar, c, 1, A.Dx);
+    ab.sxz()[c] = sxz - (tap_p(dbar + np, c, nx, A.Dz) + tap_p(dbar + 2 * np, c, 1, A.Dx));
+    ab.szz()[c] = szz - tap_m(dbar + 3 * np, c, nx, A.Dz);
+  } else {
+    ab.sxx()[c] = sxx - tap_m_b(dbar, i, j, nx, nz, 0, A.Dx);
+    ab.sxz()[c] = sxz - (tap_p_b(dbar + np, i, j, nx, nz, 1, A.Dz) + tap_p_b(dbar + 2 * np, i, j, nx, nz, 0, A.Dx));
+    ab.szz()[c] = szz - tap_m_b(dbar + 3 * np, i, j, nx, nz, 1, A.Dz);
+  }
 }
 
 // FP64 misfit: 1/2 sum (d - obs)^2 (one block, deterministic order)
@@ -682,7 +691,6 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
         case 4: k_stress_t<T, 4><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
         default: k_stress_t<T, 5><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
       }
-      k_gather_c55<T><<<gA, blk, 0, st>>>(q, g55, c.nx, c.nz);
       k_rates_t<T><<<gU, blk, 0, st>>>(A, ab, rbar);
       k_residual<T><<<(nrec + 127) / 128, 128, 0, st>>>(ab, x1, (const int2 *)p->drec, nrec, obs, nt, it, c.nx);
       k_vel_t<T><<<gU, blk, 0, st>>>(A, x0, ab, rbar, h);
@@ -691,7 +699,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
                                                                      (const T *)p->damp, shot->nsrc,
                                                                      (const T *)shot->wavelet_dev,
                                                                      shot->wavelet_nt, it, h);
-      k_gather_rho<T><<<gA, blk, 0, st>>>(h, gr, c.nx, c.nz);
+      k_gather<T><<<gA, blk, 0, st>>>(h, gr, q, g55, c.nx, c.nz);
       k_div_t<T><<<gA, blk, 0, st>>>(A, ab, rbar);
     }
   }
