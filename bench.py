@@ -287,7 +287,9 @@ def measure_serving(a, dev, seed=0):
     (gradients: iso/VTI), step counts a quarter of [1000, 8000].  The same
     arrivals are served twice: by the server with time slices given to the
     request with the least remaining work (continuous batching) and FIFO one
-    request at a time with no slicing.  Slices are 1024 steps.
+    request at a time with no slicing (one lane).  Slices are 1024 steps;
+    the continuous run has two lanes, i.e. up to two requests advancing on
+    the device at once, each on its own stream.
     Latency = submit to results in host memory (ms)."""
     import dataclasses
     import threading
@@ -322,8 +324,9 @@ def measure_serving(a, dev, seed=0):
         w = dataclasses.replace(w0, nt=nt, wavelets=w0.wavelets[:, :nt])
         reqs.append((t, grad, w))
 
-    def serve(slice_steps, max_active, policy):
-        srv = Server(device=dev.index, slice_steps=slice_steps, max_active=max_active, policy=policy)
+    def serve(slice_steps, max_active, policy, lanes):
+        srv = Server(device=dev.index, slice_steps=slice_steps, max_active=max_active, policy=policy,
+                     lanes=lanes)
         tickets = []
 
         def submitter():
@@ -362,9 +365,9 @@ def measure_serving(a, dev, seed=0):
     out = {"workload": f"{n} requests, Poisson 50/s, 70% forward / 30% gradient, grids 256^2..4096x2048, "
                        "iso/VTI/TTI (4096x2048: iso/VTI), nt 250..2000 (a quarter of 1000..8000), f32",
            "forward": sum(1 for _, g, _ in reqs if not g), "gradient": sum(1 for _, g, _ in reqs if g)}
-    runs = [("sequential", (1 << 30, 1, "shortest-first"))] + [(n_, c) for n_, c in a.serve_policies]
-    for name, (sl, ma, pol) in runs:
-        lat, wall = serve(sl, ma, pol)
+    runs = [("sequential", (1 << 30, 1, "shortest-first", 1))] + [(n_, c) for n_, c in a.serve_policies]
+    for name, (sl, ma, pol, ln) in runs:
+        lat, wall = serve(sl, ma, pol, ln)
         out[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                      "mean_ms": float(lat.mean()), "requests_per_s": n / wall, "wall_s": wall}
     out["point_steps"] = pts
@@ -553,11 +556,13 @@ def run_ours(a):
     if not a.no_grad and rank == 0:
         out["gradient"] = measure_gradient(a, dev)
     if not a.no_serve and rank == 0 and world == 1:
-        a.serve_policies = [("continuous", (1024, 64, "shortest-first"))]
+        a.serve_policies = [("continuous", (1024, 64, "shortest-first", 2))]
         if a.serve_explore:
-            a.serve_policies += [("round-robin-256", (256, 64, "round-robin")),
-                                 ("shortest-first-256", (256, 64, "shortest-first")),
-                                 ("shortest-first-4096", (4096, 64, "shortest-first"))]
+            a.serve_policies += [("one-lane", (1024, 64, "shortest-first", 1)),
+                                 ("four-lanes", (1024, 64, "shortest-first", 4)),
+                                 ("eight-lanes", (1024, 64, "shortest-first", 8)),
+                                 ("round-robin-256", (256, 64, "round-robin", 2)),
+                                 ("shortest-first-4096", (4096, 64, "shortest-first", 2))]
         out["serving"] = measure_serving(a, dev)
     if rank == 0 and world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline(w, a.cpu_seconds)

@@ -285,6 +285,10 @@ typedef struct vi_serve_config {
   int32_t max_active;       /* requests resident at once (<= 0: 64) */
   int32_t policy;           /* VI_SERVE_SHORTEST_FIRST or VI_SERVE_ROUND_ROBIN */
   int64_t hbm_budget_bytes; /* device bytes the requests may hold (<= 0: 150 GB) */
+  int32_t lanes;            /* worker threads, i.e. requests advancing on the
+                               device at once, each on its own stream
+                               (<= 0: 2; at most 16); 1 = one at a time */
+  int32_t pad_;
 } vi_serve_config;
 
 #define VI_SERVE_SHORTEST_FIRST 0 /* each slice to the request with the least work left */

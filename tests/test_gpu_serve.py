@@ -1,7 +1,8 @@
 """The request server (vi_serve): every request's results equal the direct
 call on the same inputs, alone or in a mix of grids, media and step counts
-served in round-robin slices; gradients through the server equal
-vi_gradient; HBM-budget admission; failure reporting."""
+served in slices by several lanes at once; gradients through the server
+equal vi_gradient; requests overlap on the device; HBM-budget admission;
+failure reporting."""
 import numpy as np
 import pytest
 import torch
@@ -79,6 +80,40 @@ def test_gradient_request_equals_vi_gradient(oracle_lib):
     assert np.array_equal(gt.grad, g.cpu().numpy())
     # the gradient's forward run (plain kernels) reproduces the forward solve
     assert rel_l2(gt.traces, fwd.traces) <= 1e-12
+
+
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_mix_equal_direct_calls_for_any_lane_count(lanes):
+    ws = _mix()
+    srv = Server(slice_steps=40, lanes=lanes, policy="round-robin")
+    tickets = [srv.submit_forward(w) for w in ws]
+    for t in tickets:
+        assert srv.wait(t, 120.0) == "done"
+    srv.stop()
+    for w, t in zip(ws, tickets):
+        assert np.array_equal(t.traces, _direct(w, "f32")), w.name
+
+
+def test_short_request_finishes_while_a_gradient_runs():
+    """With two lanes a small forward solve submitted while a long gradient
+    is on the device completes before the gradient does (its work overlaps
+    the gradient's instead of waiting for it)."""
+    big = media.homogeneous_iso(nx=1024, nz=512, nt=1200, pml=20, nrec=32, src=(512, 100))
+    obs = np.zeros((2, len(big.receivers), big.nt), np.float32)
+    small = media.homogeneous_iso(nx=96, nz=80, nt=60, pml=12, nrec=8, src=(40, 30))
+    srv = Server(lanes=2)
+    g = srv.submit_gradient(big, obs, "f32")
+    import time
+    t0 = time.perf_counter()
+    while srv.poll(g)[0] != "running" and time.perf_counter() - t0 < 30:
+        time.sleep(0.002)
+    time.sleep(0.02)
+    f = srv.submit_forward(small)
+    assert srv.wait(f, 60.0) == "done"
+    assert srv.poll(g)[0] == "running"
+    assert srv.wait(g, 120.0) == "done"
+    srv.stop()
+    assert np.array_equal(f.traces, _direct(small, "f32"))
 
 
 def test_budget_admission():

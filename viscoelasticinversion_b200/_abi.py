@@ -81,7 +81,8 @@ class ViShot(C.Structure):
 
 class ViServeConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("slice_steps", C.c_int32), ("max_active", C.c_int32),
-                ("policy", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+                ("policy", C.c_int32), ("hbm_budget_bytes", C.c_int64), ("lanes", C.c_int32),
+                ("pad_", C.c_int32)]
 
 
 class ViRequest(C.Structure):

@@ -9,6 +9,7 @@
 // recomputation never reads a value another CTA has already advanced.
 // Per step each cell's state and medium cross HBM once: reads of v, sigma,
 // M, psi and the medium, writes of v, sigma, M and psi.
+#include <atomic>
 #include <cstdint>
 #include <vector>
 
@@ -340,7 +341,7 @@ template <typename T, int KIND, int NSLS>
 static int launch_fused(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, cudaStream_t st) {
   using G = FusedGeom<KIND>;
   constexpr size_t smem = sizeof(T) * G::smem_elems;
-  static unsigned long long attr_set = 0;  // one bit per device
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {

@@ -9,6 +9,7 @@
 // global memory during compute.  With two stages the kernel is persistent:
 // one CTA per SM walks the tiles round-robin and the boxes of its next tile
 // load while the current tile computes.
+#include <atomic>
 #include <cudaTypedefs.h>
 
 #include "fused_tma.cuh"
@@ -760,7 +761,7 @@ static int launch_batch_one(const BatchDev<T> &b, int it, int nitems, int nsm, c
     return set_error(VI_ERR_ARG, "TMA-staged step does not fit shared memory for this medium");
   } else {
     using G = typename TmaPick<T, KIND, NSLS, PERSIST>::Lay;
-    static unsigned long long attr_set = 0;
+    static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(attr_set & (1ULL << dev))) {
@@ -813,7 +814,7 @@ static int launch_tma_one(const StepArgs<T> &a, const FusedExtras<T> &x, const T
     return set_error(VI_ERR_ARG, "TMA-staged step does not fit shared memory for this medium");
   } else {
     using G = typename TmaPick<T, KIND, NSLS, PERSIST>::Lay;
-    static unsigned long long attr_set = 0;
+    static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(attr_set & (1ULL << dev))) {

@@ -1,6 +1,7 @@
 // serve.cu — a request server over the step: forward solves and misfit
-// gradients submitted from any host thread, run by one worker thread on its
-// own CUDA stream.
+// gradients submitted from any host thread, run by a few worker threads
+// ("lanes") on one CUDA stream per resident request, so the work of
+// several requests overlaps on the device.
 //
 // The reference solves one problem per call and has no server
 // (sciml_solver/ViscoelasticProblem.jl:273-309).  Scheduling here:
@@ -14,7 +15,12 @@
 //    gradient), so a short request that arrives while a long one runs
 //    preempts it at the next slice boundary (shortest remaining work
 //    first, which minimises mean latency);
-//  * gradient requests run whole when their turn comes (one vi_gradient).
+//  * gradient requests run whole when their turn comes (one vi_gradient);
+//  * lanes: each lane takes the next slice of the best idle resident
+//    request and issues it on that request's stream; with L lanes the L
+//    requests with the least remaining work advance at the same time (a
+//    gradient occupies one lane while the others keep the forward solves
+//    going, small grids run beside large ones).
 // Each request has its own plan and device buffers, so its results do not
 // depend on what else is resident (the sliced stepping is bitwise equal to
 // one vi_step call).  Latency is measured from submit to the moment the
@@ -47,7 +53,7 @@ struct Req {
   std::string msg;
   Clock::time_point t_submit, t_done;
   int64_t footprint = 0;
-  // resident state (worker thread only)
+  // resident state (used by the lane that holds the request)
   vi_plan *plan = nullptr;
   void *buf = nullptr;
   vi_medium md{};
@@ -56,6 +62,9 @@ struct Req {
   void *obs_dev = nullptr;
   double *grad_dev = nullptr;
   int done_steps = 0;
+  cudaStream_t st = nullptr;  // the request's own stream: its slices stay in order
+  bool busy = false;          // a lane is advancing it (under the server lock)
+  uint64_t last_turn = 0;     // round robin: when it last got a slice
 };
 
 size_t esize_of(const vi_config &c) { return c.precision == VI_F64 ? 8 : 4; }
@@ -99,16 +108,17 @@ using namespace vb;
 
 struct vi_server {
   vi_serve_config cfg{};
-  std::thread worker;
+  std::vector<std::thread> lanes;
   std::mutex mu;
   std::condition_variable cv;
   std::deque<std::shared_ptr<Req>> queue;
-  std::vector<std::shared_ptr<Req>> active;
+  std::vector<std::shared_ptr<Req>> active;  // resident (admitted and staged)
   std::unordered_map<uint64_t, std::shared_ptr<Req>> all;
   uint64_t next_ticket = 1;
+  uint64_t turn = 0;
+  int admitting = 0;  // admitted, still being staged by a lane
   bool stopping = false;
   int64_t used = 0;
-  cudaStream_t st = nullptr;
 };
 
 namespace {
@@ -118,8 +128,9 @@ int admit_impl(vi_server *s, Req &q) {
   const vi_request &r = q.rq;
   const vi_config &c = r.cfg;
   const size_t np = (size_t)c.nx * c.nz;
-  int rc = vi_plan_create(&c, &q.plan);
+  int rc = cuda_check(cudaStreamCreateWithFlags(&q.st, cudaStreamNonBlocking), "serve: create stream");
   if (rc) return rc;
+  if ((rc = vi_plan_create(&c, &q.plan))) return rc;
   const int ns = 5 + 3 * c.nsls;
   const int nmed = 8;
   const size_t tr = 2 * (size_t)r.nrec * r.nt;
@@ -136,14 +147,14 @@ int admit_impl(vi_server *s, Req &q) {
     *dp[k] = nullptr;
     if (hp[k]) {
       T *d = base + k * np;
-      if ((rc = cuda_check(cudaMemcpyAsync(d, hp[k], np * sizeof(T), cudaMemcpyHostToDevice, s->st),
+      if ((rc = cuda_check(cudaMemcpyAsync(d, hp[k], np * sizeof(T), cudaMemcpyHostToDevice, q.st),
                            "serve: upload medium")))
         return rc;
       *dp[k] = d;
     }
   }
   T *state = base + nmed * np;
-  if ((rc = cuda_check(cudaMemsetAsync(state, 0, ns * np * sizeof(T), s->st), "serve: zero state"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(state, 0, ns * np * sizeof(T), q.st), "serve: zero state"))) return rc;
   q.fd.vx = state;
   q.fd.vz = state + np;
   q.fd.sxx = state + 2 * np;
@@ -153,13 +164,13 @@ int admit_impl(vi_server *s, Req &q) {
   q.fd.m_plane_stride = (long long)np;
   T *w = state + ns * np;
   T *t = w + wav;
-  if (wav && (rc = cuda_check(cudaMemcpyAsync(w, r.wavelet_host, wav * sizeof(T), cudaMemcpyHostToDevice, s->st),
+  if (wav && (rc = cuda_check(cudaMemcpyAsync(w, r.wavelet_host, wav * sizeof(T), cudaMemcpyHostToDevice, q.st),
                               "serve: upload wavelets")))
     return rc;
-  if (tr && (rc = cuda_check(cudaMemsetAsync(t, 0, tr * sizeof(T), s->st), "serve: zero traces"))) return rc;
+  if (tr && (rc = cuda_check(cudaMemsetAsync(t, 0, tr * sizeof(T), q.st), "serve: zero traces"))) return rc;
   if (grad) {
     T *o = t + tr;
-    if ((rc = cuda_check(cudaMemcpyAsync(o, r.obs_host, tr * sizeof(T), cudaMemcpyHostToDevice, s->st),
+    if ((rc = cuda_check(cudaMemcpyAsync(o, r.obs_host, tr * sizeof(T), cudaMemcpyHostToDevice, q.st),
                          "serve: upload observed traces")))
       return rc;
     q.obs_dev = o;
@@ -174,8 +185,8 @@ int admit_impl(vi_server *s, Req &q) {
   q.shot.rec_host = q.rec.empty() ? nullptr : q.rec.data();
   q.shot.traces_dev = t;
   q.shot.traces_nt = r.nt;
-  if ((rc = vi_plan_reset(q.plan, s->st))) return rc;
-  return cuda_check(cudaStreamSynchronize(s->st), "serve: stage request");
+  if ((rc = vi_plan_reset(q.plan, q.st))) return rc;
+  return cuda_check(cudaStreamSynchronize(q.st), "serve: stage request");
 }
 
 int admit(vi_server *s, Req &q) {
@@ -183,10 +194,13 @@ int admit(vi_server *s, Req &q) {
 }
 
 void release(Req &q) {
+  if (q.st) cudaStreamSynchronize(q.st);
   if (q.plan) vi_plan_destroy(q.plan);
   q.plan = nullptr;
   if (q.buf) cudaFree(q.buf);
   q.buf = nullptr;
+  if (q.st) cudaStreamDestroy(q.st);
+  q.st = nullptr;
 }
 
 // Runs the request's next slice (forward) or all of it (gradient); returns
@@ -197,30 +211,30 @@ int advance(vi_server *s, Req &q, bool *finished) {
   int rc;
   if (r.kind == VI_REQ_GRADIENT) {
     double J = 0;
-    if ((rc = vi_gradient(q.plan, &q.md, &q.shot, r.nt, q.obs_dev, 0, 0, q.grad_dev, &J, s->st))) return rc;
+    if ((rc = vi_gradient(q.plan, &q.md, &q.shot, r.nt, q.obs_dev, 0, 0, q.grad_dev, &J, q.st))) return rc;
     const size_t np = (size_t)r.cfg.nx * r.cfg.nz;
     if ((rc = cuda_check(cudaMemcpyAsync(r.grad_host, q.grad_dev, 8 * np * sizeof(double), cudaMemcpyDeviceToHost,
-                                         s->st),
+                                         q.st),
                          "serve: download gradient")))
       return rc;
     if (r.misfit_host) *r.misfit_host = J;
   } else {
     int n = s->cfg.slice_steps;
     if (n > r.nt - q.done_steps) n = r.nt - q.done_steps;
-    if ((rc = vi_step(q.plan, &q.md, &q.fd, &q.shot, q.done_steps, n, 0, s->st))) return rc;
+    if ((rc = vi_step(q.plan, &q.md, &q.fd, &q.shot, q.done_steps, n, 0, q.st))) return rc;
     q.done_steps += n;
     if (q.done_steps < r.nt) {
       *finished = false;
       return VI_OK;
     }
-    if ((rc = vi_plan_status(q.plan, s->st))) return rc;
+    if ((rc = vi_plan_status(q.plan, q.st))) return rc;
   }
   const size_t tr = 2 * (size_t)r.nrec * r.nt;
   if (tr && r.traces_host &&
-      (rc = cuda_check(cudaMemcpyAsync(r.traces_host, q.shot.traces_dev, tr * es, cudaMemcpyDeviceToHost, s->st),
+      (rc = cuda_check(cudaMemcpyAsync(r.traces_host, q.shot.traces_dev, tr * es, cudaMemcpyDeviceToHost, q.st),
                        "serve: download traces")))
     return rc;
-  if ((rc = cuda_check(cudaStreamSynchronize(s->st), "serve: finish request"))) return rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(q.st), "serve: finish request"))) return rc;
   *finished = true;
   return VI_OK;
 }
@@ -236,54 +250,88 @@ void finish(vi_server *s, const std::shared_ptr<Req> &q, int rc) {
   s->cv.notify_all();
 }
 
-void worker_main(vi_server *s) {
+// true when the front of the queue may be admitted now
+bool can_admit(const vi_server *s) {
+  return !s->queue.empty() && (int)s->active.size() + s->admitting < s->cfg.max_active &&
+         s->used + s->queue.front()->footprint <= s->cfg.hbm_budget_bytes;
+}
+
+// the idle resident request the policy picks next (nullptr if none)
+std::shared_ptr<Req> pick_idle(vi_server *s) {
+  std::shared_ptr<Req> best;
+  for (auto &q : s->active) {
+    if (q->busy) continue;
+    if (!best) {
+      best = q;
+    } else if (s->cfg.policy == VI_SERVE_ROUND_ROBIN ? q->last_turn < best->last_turn
+                                                      : remaining_work(*q) < remaining_work(*best)) {
+      best = q;
+    }
+  }
+  return best;
+}
+
+bool any_idle(const vi_server *s) {
+  for (auto &q : s->active)
+    if (!q->busy) return true;
+  return false;
+}
+
+void lane_main(vi_server *s) {
   cudaSetDevice(s->cfg.device);
   for (;;) {
-    std::vector<std::shared_ptr<Req>> admitted;
+    std::shared_ptr<Req> adm, pick;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      // wait for work unless requests are resident
-      s->cv.wait(lk, [&] { return s->stopping || !s->queue.empty() || !s->active.empty(); });
-      while (!s->queue.empty() && (int)s->active.size() + (int)admitted.size() < s->cfg.max_active &&
-             s->used + s->queue.front()->footprint <= s->cfg.hbm_budget_bytes) {
-        auto q = s->queue.front();
+      const auto drained = [&] {
+        return s->stopping && s->queue.empty() && s->active.empty() && s->admitting == 0;
+      };
+      s->cv.wait(lk, [&] { return can_admit(s) || any_idle(s) || drained(); });
+      if (can_admit(s)) {
+        adm = s->queue.front();
         s->queue.pop_front();
-        s->used += q->footprint;
-        q->state = VI_REQ_RUNNING;
-        admitted.push_back(q);
+        s->used += adm->footprint;
+        adm->state = VI_REQ_RUNNING;
+        ++s->admitting;
+      } else if ((pick = pick_idle(s))) {
+        pick->busy = true;
+        pick->last_turn = ++s->turn;
+      } else {
+        return;  // drained
       }
-      if (s->stopping && s->queue.empty() && s->active.empty() && admitted.empty()) return;
     }
-    for (auto &q : admitted) {
-      const int rc = admit(s, *q);
+    if (adm) {
+      const int rc = admit(s, *adm);
       if (rc) {
-        finish(s, q, rc);
+        {
+          std::lock_guard<std::mutex> lk(s->mu);
+          --s->admitting;
+        }
+        finish(s, adm, rc);
         continue;
       }
-      s->active.push_back(q);  // worker-owned list
+      std::lock_guard<std::mutex> lk(s->mu);
+      --s->admitting;
+      s->active.push_back(adm);
+      s->cv.notify_all();
+      continue;
     }
-    if (s->active.empty()) continue;
-    std::vector<std::shared_ptr<Req>> picks;
-    if (s->cfg.policy == VI_SERVE_ROUND_ROBIN) {
-      picks = s->active;  // one slice each
-    } else {  // one slice for the resident request with the least remaining work
-      size_t best = 0;
-      for (size_t k = 1; k < s->active.size(); ++k)
-        if (remaining_work(*s->active[k]) < remaining_work(*s->active[best])) best = k;
-      picks.push_back(s->active[best]);
-    }
-    for (auto &q : picks) {
-      bool fin = false;
-      const int rc = advance(s, *q, &fin);
-      if (rc || fin) {
-        finish(s, q, rc);
+    bool fin = false;
+    const int rc = advance(s, *pick, &fin);
+    if (rc || fin) {
+      {
         std::lock_guard<std::mutex> lk(s->mu);
         for (size_t k = 0; k < s->active.size(); ++k)
-          if (s->active[k] == q) {
+          if (s->active[k] == pick) {
             s->active.erase(s->active.begin() + (long)k);
             break;
           }
       }
+      finish(s, pick, rc);
+    } else {
+      std::lock_guard<std::mutex> lk(s->mu);
+      pick->busy = false;
+      s->cv.notify_all();
     }
   }
 }
@@ -302,12 +350,16 @@ extern "C" int vi_serve_start(const vi_serve_config *cfg, vi_server **out) {
   if (s->cfg.max_active <= 0) s->cfg.max_active = 64;
   if (s->cfg.hbm_budget_bytes <= 0) s->cfg.hbm_budget_bytes = 150LL * 1000 * 1000 * 1000;
   if (s->cfg.policy != VI_SERVE_ROUND_ROBIN) s->cfg.policy = VI_SERVE_SHORTEST_FIRST;
-  if ((rc = cuda_check(cudaSetDevice(cfg->device), "cudaSetDevice")) ||
-      (rc = cuda_check(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "serve: create stream"))) {
+  // two lanes measured best on the mixed request stream (one for the long
+  // solves, one for the short ones; more lanes make the large solves share
+  // the GPU with each other)
+  if (s->cfg.lanes <= 0) s->cfg.lanes = 2;
+  if (s->cfg.lanes > 16) s->cfg.lanes = 16;
+  if ((rc = cuda_check(cudaSetDevice(cfg->device), "cudaSetDevice"))) {
     delete s;
     return rc;
   }
-  s->worker = std::thread(worker_main, s);
+  for (int k = 0; k < s->cfg.lanes; ++k) s->lanes.emplace_back(lane_main, s);
   *out = s;
   return VI_OK;
 }
@@ -379,9 +431,8 @@ extern "C" int vi_serve_stop(vi_server *s) {
     s->stopping = true;
     s->cv.notify_all();
   }
-  if (s->worker.joinable()) s->worker.join();
-  cudaSetDevice(s->cfg.device);
-  if (s->st) cudaStreamDestroy(s->st);
+  for (auto &t : s->lanes)
+    if (t.joinable()) t.join();
   delete s;
   return VI_OK;
 }

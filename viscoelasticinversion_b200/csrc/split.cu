@@ -30,6 +30,7 @@
 // M and psi only at its own cells.  The TTI stress pass also reads M and
 // psi on a ring of neighbouring cells, so for TTI those two ping-pong
 // between buffers every step (sigma and v stay in place).
+#include <atomic>
 #include <cudaTypedefs.h>
 
 #include <cstdint>
@@ -490,7 +491,7 @@ template <typename T, int KIND, int NSLS>
 static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                          int ntiles, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
@@ -543,7 +544,7 @@ int launch_split_vel_batch(int kind, const BatchDev<T> &b, int it, int nitems, c
 template <typename T, int KIND, int NSLS>
 static int launch_stress_batch(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
@@ -592,7 +593,7 @@ static int launch_vel_tma(const StepArgs<T> &a, const FusedExtras<T> &x, const S
                           int ntiles, cudaStream_t st, bool pdl) {
   using G = SplitVelTma<T>;
   const bool pp = a.psix_o != a.psix || a.psiz_o != a.psiz;
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {

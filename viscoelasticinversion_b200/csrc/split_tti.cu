@@ -11,6 +11,7 @@
 // buffer and written to the other (ping-pong per step); sigma is read and
 // written only at the CTA's own cells, in place.  The velocity pass is the
 // medium-independent k_split_vel_ldg.
+#include <atomic>
 #include <cudaTypedefs.h>
 
 #include <cstdint>
@@ -307,7 +308,7 @@ template <typename T, int NSLS>
 static int launch_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
                       cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
@@ -338,7 +339,7 @@ int launch_split_stress_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const
 template <typename T, int NSLS>
 static int launch_tti_batch(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {

@@ -28,6 +28,7 @@
 // read and written by their owner only and stay in place.  CPML psi
 // ping-pongs between the plan's two sets.  Bounded mbarrier waits report
 // through the plan's error word.
+#include <atomic>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -523,7 +524,7 @@ template <int KIND, int NSLS>
 static int launch_stream_k(const StepArgs<float> &a, const StreamExtras &x, const StreamMaps &m, int nsm,
                            cudaStream_t st, bool pdl) {
   using LY = SLayout<KIND, NSLS>;
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   static int grid_per_dev[64] = {0};
   int dev = 0;
   cudaGetDevice(&dev);

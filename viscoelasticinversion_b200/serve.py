@@ -1,10 +1,11 @@
 """Request server over the vi_serve C ABI.
 
 Forward solves and misfit gradients are submitted from host code and run
-by the library's worker thread: admission against an HBM budget, time
-slices of slice_steps steps given to the resident request with the least
-remaining work (requests join and leave between slices, short ones preempt
-long ones), gradients run whole.  The reference solves one
+by the library's worker lanes: admission against an HBM budget, time
+slices of slice_steps steps given to the idle resident requests with the
+least remaining work (requests join and leave between slices, short ones
+preempt long ones), gradients run whole, and `lanes` requests advance on
+the device at once, each on its own CUDA stream.  The reference solves one
 problem per call (sciml_solver/ViscoelasticProblem.jl:273-309); this is
 its time step served to many callers.
 """
@@ -36,10 +37,12 @@ class Ticket:
 
 class Server:
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slice_steps: int = 1024,
-                 max_active: int = 64, policy: str = "shortest-first"):
+                 max_active: int = 64, policy: str = "shortest-first", lanes: int = 2):
+        """lanes: requests advancing on the device at once (each resident
+        request has its own CUDA stream; 1 = one at a time)."""
         pol = {"shortest-first": 0, "round-robin": 1}[policy]
         cfg = ViServeConfig(device=device, slice_steps=slice_steps, max_active=max_active,
-                            policy=pol, hbm_budget_bytes=hbm_budget_bytes)
+                            policy=pol, hbm_budget_bytes=hbm_budget_bytes, lanes=lanes)
         self._h = C.c_void_p()
         check(lib().vi_serve_start(C.byref(cfg), C.byref(self._h)))
 
