@@ -109,6 +109,11 @@ using namespace vb;
 struct vi_server {
   vi_serve_config cfg{};
   std::vector<std::thread> lanes;
+  // plans of finished requests, reused by later requests with the same
+  // configuration (destroying a plan frees device memory, which
+  // synchronises the whole device and would stall the other lanes)
+  std::mutex plan_mu;
+  std::vector<vi_plan *> plan_cache;
   std::mutex mu;
   std::condition_variable cv;
   std::deque<std::shared_ptr<Req>> queue;
@@ -123,6 +128,40 @@ struct vi_server {
 
 namespace {
 
+constexpr size_t kPlanCache = 8;
+
+bool same_config(const vi_config &a, const vi_config &b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+
+// A plan for config c: a cached one when there is one, else a new one.
+int take_plan(vi_server *s, const vi_config &c, vi_plan **out) {
+  {
+    std::lock_guard<std::mutex> lk(s->plan_mu);
+    for (size_t k = 0; k < s->plan_cache.size(); ++k) {
+      vi_plan *p = s->plan_cache[k];
+      if (same_config(p->cfg, c)) {
+        s->plan_cache.erase(s->plan_cache.begin() + (long)k);
+        *out = p;
+        return VI_OK;
+      }
+    }
+  }
+  return vi_plan_create(&c, out);
+}
+
+// Keeps a finished request's plan for reuse (oldest evicted beyond the cap).
+void give_plan(vi_server *s, vi_plan *p) {
+  vi_plan *evict = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(s->plan_mu);
+    s->plan_cache.push_back(p);
+    if (s->plan_cache.size() > kPlanCache) {
+      evict = s->plan_cache.front();
+      s->plan_cache.erase(s->plan_cache.begin());
+    }
+  }
+  if (evict) vi_plan_destroy(evict);
+}
+
 template <typename T>
 int admit_impl(vi_server *s, Req &q) {
   const vi_request &r = q.rq;
@@ -130,7 +169,7 @@ int admit_impl(vi_server *s, Req &q) {
   const size_t np = (size_t)c.nx * c.nz;
   int rc = cuda_check(cudaStreamCreateWithFlags(&q.st, cudaStreamNonBlocking), "serve: create stream");
   if (rc) return rc;
-  if ((rc = vi_plan_create(&c, &q.plan))) return rc;
+  if ((rc = take_plan(s, c, &q.plan))) return rc;
   const int ns = 5 + 3 * c.nsls;
   const int nmed = 8;
   const size_t tr = 2 * (size_t)r.nrec * r.nt;
@@ -138,7 +177,8 @@ int admit_impl(vi_server *s, Req &q) {
   const bool grad = r.kind == VI_REQ_GRADIENT;
   size_t elems = (nmed + ns) * np + wav + tr + (grad ? tr : 0) + 64;
   size_t bytes = elems * sizeof(T) + (grad ? 8 * np * sizeof(double) + 256 : 0);
-  if ((rc = cuda_check(cudaMalloc(&q.buf, bytes), "serve: allocate request buffers"))) return rc;
+  // stream-ordered: no device-wide synchronisation, so other lanes run on
+  if ((rc = cuda_check(cudaMallocAsync(&q.buf, bytes, q.st), "serve: allocate request buffers"))) return rc;
   T *base = (T *)q.buf;
   const void *hp[8] = {r.medium_host.rho, r.medium_host.c11, r.medium_host.c13, r.medium_host.c15,
                        r.medium_host.c33, r.medium_host.c35, r.medium_host.c55, r.medium_host.tau};
@@ -193,12 +233,12 @@ int admit(vi_server *s, Req &q) {
   return q.rq.cfg.precision == VI_F64 ? admit_impl<double>(s, q) : admit_impl<float>(s, q);
 }
 
-void release(Req &q) {
-  if (q.st) cudaStreamSynchronize(q.st);
-  if (q.plan) vi_plan_destroy(q.plan);
-  q.plan = nullptr;
-  if (q.buf) cudaFree(q.buf);
+void release(vi_server *s, Req &q) {
+  if (q.buf) cudaFreeAsync(q.buf, q.st);
   q.buf = nullptr;
+  if (q.st) cudaStreamSynchronize(q.st);
+  if (q.plan) give_plan(s, q.plan);
+  q.plan = nullptr;
   if (q.st) cudaStreamDestroy(q.st);
   q.st = nullptr;
 }
@@ -240,7 +280,7 @@ int advance(vi_server *s, Req &q, bool *finished) {
 }
 
 void finish(vi_server *s, const std::shared_ptr<Req> &q, int rc) {
-  release(*q);
+  release(s, *q);
   std::lock_guard<std::mutex> lk(s->mu);
   q->err = rc;
   if (rc) q->msg = vi_last_error();
@@ -433,6 +473,7 @@ extern "C" int vi_serve_stop(vi_server *s) {
   }
   for (auto &t : s->lanes)
     if (t.joinable()) t.join();
+  for (vi_plan *p : s->plan_cache) vi_plan_destroy(p);
   delete s;
   return VI_OK;
 }
