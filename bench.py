@@ -205,18 +205,26 @@ def run_reference(a):
     }), flush=True)
 
 
-def measure_batch(a, dev, stream, max_over_ranks, barrier, world):
+SMALL_GRIDS = ((256, 256), (384, 256), (512, 256))
+
+
+def measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=False):
     """Shots/s of the batched TTI gather (64 shots, grids from {512²,
     1024x512, 1536x768, 2048x1024}, nt in [1500, 4000], one CUDA graph)
-    against the plain path (the same fused TMA kernel, one shot after the
-    other, one launch per step, no graph).  Each rank runs its own gather."""
+    against the plain path (the kernel form the tuner picked, one shot
+    after the other, launched step by step, no graph).  small: the same
+    with grids from {256², 384x256, 512x256}, where one shot does not fill
+    the GPU.  Each rank runs its own gather."""
     import torch
 
     from viscoelasticinversion_b200 import StepPlan, media
     from viscoelasticinversion_b200.batch import ShotBatch
 
     rank = int(os.environ.get("RANK", "0"))
-    ws = media.shot_gather(a.batch_shots, seed=rank, kind="tti")
+    if small:
+        ws = media.shot_gather(a.batch_shots, seed=rank, kind="tti", grids=SMALL_GRIDS, pml=20)
+    else:
+        ws = media.shot_gather(a.batch_shots, seed=rank, kind="tti")
     b = ShotBatch(ws, "f32", device=dev.index)
     b.run()  # tunes the kernel form, captures the graph, runs once
     b.reset()
@@ -267,7 +275,8 @@ def measure_batch(a, dev, stream, max_over_ranks, barrier, world):
     n = len(ws)
     for c in per_class.values():
         c["plain_gpts"] = c["point_steps"] / (c["plain_ms"] / 1e3) / 1e9
-    out = {"workload": f"tti-gather-{n}shots-grids512..2048x1024-nt1500..4000-f32",
+    grids = "256x256..512x256-cpml20" if small else "512..2048x1024"
+    out = {"workload": f"tti-gather-{n}shots-grids{grids}-nt1500..4000-f32",
            "shots": n * world, "kernel_form": form,
            "batched_ms": batched_ms, "plain_ms": plain_ms,
            "batched_shots_per_s": n * world / (batched_ms / 1e3),
@@ -555,6 +564,7 @@ def run_ours(a):
 
     if not a.no_batch:
         out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
+        out["batched_small"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=True)
     if not a.no_grad and rank == 0:
         out["gradient"] = measure_gradient(a, dev)
     if not a.no_serve and rank == 0 and world == 1:
