@@ -29,6 +29,7 @@
 
 #include "fused.cuh"
 #include "fused_tma.cuh"
+#include "pdl.cuh"
 #include "plain.cuh"
 #include "plan.cuh"
 #include "split.cuh"
@@ -128,6 +129,7 @@ __device__ __forceinline__ T cpml_fwd(T d, T p0, T a, T b, T ik, T *pn) {
 // target rows are distinct, so the read-modify-writes need not serialise)
 template <typename T>
 __global__ void k_mirror_t(T *sb_zz, T *sb_xz, int nx) {
+  pdl_wait();  // launched while the previous kernel drains
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nx) return;
   T gz[L], tz[L], gq[L], tq[L];
@@ -162,6 +164,7 @@ template <typename T, int N>
 __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot<T> x1, Slot<T> ab,
                                                    T *rbar, T *q, double *gc11, double *gc13,
                                                    double *gc33, double *gtau) {
+  pdl_wait();  // launched while the previous kernel drains
   constexpr int NM = N > 0 ? N : 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
@@ -298,6 +301,7 @@ __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot
 // so they stay inside the planes; rbar is zero outside the region)
 template <typename T>
 __global__ void k_rates_t(AdjArgs<T> A, Slot<T> ab, const T *rbar) {
+  pdl_wait();  // launched while the previous kernel drains
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
   if (i >= A.nx - L || j >= A.nz - L) return;
@@ -312,6 +316,7 @@ __global__ void k_rates_t(AdjArgs<T> A, Slot<T> ab, const T *rbar) {
 template <typename T>
 __global__ void k_residual(Slot<T> ab, Slot<T> x1, const int2 *rec, int nrec, const T *obs, int ont,
                            int it, int nx) {
+  pdl_wait();  // launched while the previous kernel drains
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nrec) return;
   const long long c = (long long)rec[r].y * nx + rec[r].x;
@@ -323,6 +328,7 @@ __global__ void k_residual(Slot<T> ab, Slot<T> x1, const int2 *rec, int nrec, co
 // buoyancy-gradient terms h (2 planes)
 template <typename T>
 __global__ void __launch_bounds__(256) k_vel_t(AdjArgs<T> A, Slot<T> x0, Slot<T> ab, T *dbar, T *h) {
+  pdl_wait();  // launched while the previous kernel drains
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
   if (i >= A.nx - L || j >= A.nz - L) return;
@@ -380,6 +386,7 @@ __global__ void __launch_bounds__(256) k_vel_t(AdjArgs<T> A, Slot<T> x0, Slot<T>
 template <typename T>
 __global__ void k_force_rho_t(AdjArgs<T> A, Slot<T> ab, const int4 *src, const T *amp, int nsrc,
                               const T *wav, int wnt, int it, T *h) {
+  pdl_wait();  // launched while the previous kernel drains
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsrc) return;
   const int4 s = src[q];
@@ -399,6 +406,7 @@ __global__ void k_force_rho_t(AdjArgs<T> A, Slot<T> ab, const int4 *src, const T
 // gc55 gathers the 4 half-node terms q that average mu around each cell
 template <typename T>
 __global__ void k_gather(const T *h, double *grho, const T *q, double *gc55, int nx, int nz) {
+  pdl_wait();  // launched while the previous kernel drains
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= nx || j >= nz) return;
   const long long c = (long long)j * nx + i, np = (long long)nx * nz;
@@ -420,6 +428,7 @@ __global__ void k_gather(const T *h, double *grho, const T *q, double *gc55, int
 // included; the images^T of the previous step folds them)
 template <typename T>
 __global__ void k_div_t(AdjArgs<T> A, Slot<T> ab, const T *dbar) {
+  pdl_wait();  // launched while the previous kernel drains
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= A.nx || j >= A.nz) return;
   const int nx = A.nx, nz = A.nz;
@@ -667,6 +676,11 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   const dim3 blk(32, 8);
   const dim3 gU((c.nx - 2 * L + 31) / 32, (c.nz - 2 * L + 7) / 8);
   const dim3 gA((c.nx + 31) / 32, (c.nz + 7) / 8);
+  int lrc = VI_OK;  // first launch error of the adjoint sweep
+  auto lc = [&](auto kernel, dim3 g, dim3 b, auto... args) {
+    const cudaError_t e = launch_pdl(kernel, g, b, 0, st, true, args...);
+    if (e != cudaSuccess && !lrc) lrc = cuda_check(e, "adjoint launch");
+  };
   for (int qseg = nck - 1; qseg >= 0; --qseg) {
     const int s0 = qseg * K, s1 = std::min(nt, s0 + K);
     // recompute the segment: seg[k] = state before step s0 + k
@@ -682,27 +696,28 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     }
     for (int it = s1 - 1; it >= s0; --it) {
       const Slot<T> x0 = mk(seg + (size_t)(it - s0) * slot), x1 = mk(seg + (size_t)(it - s0 + 1) * slot);
-      if (c.free_surface) k_mirror_t<T><<<(c.nx + 127) / 128, 128, 0, st>>>(ab.szz(), ab.sxz(), c.nx);
+      // every kernel of the step overlaps its predecessor's tail and waits
+      // for it at entry (programmatic dependent launch)
+      if (c.free_surface) lc(k_mirror_t<T>, dim3((c.nx + 127) / 128), dim3(128), ab.szz(), ab.sxz(), c.nx);
       switch (N) {
-        case 0: k_stress_t<T, 0><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
-        case 1: k_stress_t<T, 1><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
-        case 2: k_stress_t<T, 2><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
-        case 3: k_stress_t<T, 3><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
-        case 4: k_stress_t<T, 4><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
-        default: k_stress_t<T, 5><<<gU, blk, 0, st>>>(A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 0: lc(k_stress_t<T, 0>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 1: lc(k_stress_t<T, 1>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 2: lc(k_stress_t<T, 2>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 3: lc(k_stress_t<T, 3>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        case 4: lc(k_stress_t<T, 4>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
+        default: lc(k_stress_t<T, 5>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
       }
-      k_rates_t<T><<<gU, blk, 0, st>>>(A, ab, rbar);
-      k_residual<T><<<(nrec + 127) / 128, 128, 0, st>>>(ab, x1, (const int2 *)p->drec, nrec, obs, nt, it, c.nx);
-      k_vel_t<T><<<gU, blk, 0, st>>>(A, x0, ab, rbar, h);
+      lc(k_rates_t<T>, gU, blk, A, ab, (const T *)rbar);
+      lc(k_residual<T>, dim3((nrec + 127) / 128), dim3(128), ab, x1, (const int2 *)p->drec, nrec, obs, nt, it, c.nx);
+      lc(k_vel_t<T>, gU, blk, A, x0, ab, rbar, h);
       if (shot->nsrc > 0)
-        k_force_rho_t<T><<<(shot->nsrc + 127) / 128, 128, 0, st>>>(A, ab, (const int4 *)p->dsrc,
-                                                                     (const T *)p->damp, shot->nsrc,
-                                                                     (const T *)shot->wavelet_dev,
-                                                                     shot->wavelet_nt, it, h);
-      k_gather<T><<<gA, blk, 0, st>>>(h, gr, q, g55, c.nx, c.nz);
-      k_div_t<T><<<gA, blk, 0, st>>>(A, ab, rbar);
+        lc(k_force_rho_t<T>, dim3((shot->nsrc + 127) / 128), dim3(128), A, ab, (const int4 *)p->dsrc,
+           (const T *)p->damp, shot->nsrc, (const T *)shot->wavelet_dev, shot->wavelet_nt, it, h);
+      lc(k_gather<T>, gA, blk, (const T *)h, gr, (const T *)q, g55, c.nx, c.nz);
+      lc(k_div_t<T>, gA, blk, A, ab, (const T *)rbar);
     }
   }
+  if (lrc) return lrc;
   if (c.medium == VI_MEDIUM_ISO) k_fold_iso<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(np, grad);
   p->last_kernel = 1;
   if ((rc = cuda_check(cudaGetLastError(), "gradient launch"))) return rc;
