@@ -614,7 +614,9 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     fxs.ntx = sntx_keep;
     fxs.tile_off = soff_keep;
   }
-  auto fwd_step = [&](const Slot<T> &sl, int it, T *traces, bool pdl) -> int {
+  // One forward step of slot sl, in place, or (split pair, out != nullptr)
+  // from slot sl into slot *out, which then holds the next state.
+  auto fwd_step = [&](const Slot<T> &sl, int it, T *traces, bool pdl, const Slot<T> *out = nullptr) -> int {
     if (!use_split) {
       bind(a, sl);
       x.traces = traces;
@@ -623,17 +625,28 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     }
     StepArgs<T> b = a;
     bind(b, sl);
+    if (out) {
+      b.vx_o = out->vx(); b.vz_o = out->vz();
+      b.sxx_o = out->sxx(); b.szz_o = out->szz(); b.sxz_o = out->sxz();
+      b.m_o = out->m(); b.mstride_o = np;
+      b.psix_o = p->wx ? out->psix() : nullptr;
+      b.psiz_o = p->hz ? out->psiz() : nullptr;
+    }
     fx.it = fxs.it = it;
     fx.traces = fxs.traces = traces;
-    int r2 = encode_map(&ms.a, b.vx, (int)sizeof(T), c.nx, c.nz, 1, 0, SS::BW, SS::BH, 1);
-    if (!r2) r2 = encode_map(&ms.b, b.vz, (int)sizeof(T), c.nx, c.nz, 1, 0, SS::BW, SS::BH, 1);
+    // the stress pass stages the new velocities: those of the output state
+    T *nvx = out ? out->vx() : b.vx, *nvz = out ? out->vz() : b.vz;
+    int r2 = encode_map(&ms.a, nvx, (int)sizeof(T), c.nx, c.nz, 1, 0, SS::BW, SS::BH, 1);
+    if (!r2) r2 = encode_map(&ms.b, nvz, (int)sizeof(T), c.nx, c.nz, 1, 0, SS::BW, SS::BH, 1);
     if (!r2) r2 = launch_split_vel<T>(b, fx, ntiles, st, pdl);
     if (!r2) r2 = launch_split_stress<T>(c.medium, b, fxs, ms, sntiles, st, true);
     return r2;
   };
   // ---- forward sweep with checkpoints and traces ----
   Slot<T> cur = mk(seg);
-  if ((rc = cuda_check(cudaMemsetAsync(seg, 0, sbytes, st), "zero state"))) return rc;
+  // every segment slot starts at zero: cells the kernels never write (outside
+  // the update region, off the CPML strips) stay zero in all of them
+  if ((rc = cuda_check(cudaMemsetAsync(seg, 0, (size_t)(K + 1) * sbytes, st), "zero segment"))) return rc;
   for (int it = 0; it < nt; ++it) {
     if (it % K == 0)
       if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, seg, sbytes, cudaMemcpyDeviceToDevice, st),
@@ -689,10 +702,16 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
       return rc;
     for (int k = 0; k < s1 - s0; ++k) {
       T *nxt = seg + (size_t)(k + 1) * slot;
-      if ((rc = cuda_check(cudaMemcpyAsync(nxt, seg + (size_t)k * slot, sbytes, cudaMemcpyDeviceToDevice, st),
-                           "segment copy")))
-        return rc;
-      if ((rc = fwd_step(mk(nxt), s0 + k, nullptr, false))) return rc;
+      if (use_split) {
+        // straight from slot k into slot k + 1 (no copy of the state)
+        const Slot<T> out = mk(nxt);
+        if ((rc = fwd_step(mk(seg + (size_t)k * slot), s0 + k, nullptr, k > 0, &out))) return rc;
+      } else {
+        if ((rc = cuda_check(cudaMemcpyAsync(nxt, seg + (size_t)k * slot, sbytes, cudaMemcpyDeviceToDevice, st),
+                             "segment copy")))
+          return rc;
+        if ((rc = fwd_step(mk(nxt), s0 + k, nullptr, false))) return rc;
+      }
     }
     for (int it = s1 - 1; it >= s0; --it) {
       const Slot<T> x0 = mk(seg + (size_t)(it - s0) * slot), x1 = mk(seg + (size_t)(it - s0 + 1) * slot);

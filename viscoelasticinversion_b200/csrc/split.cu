@@ -55,7 +55,9 @@ namespace vb {
 // CPML, buoyancy, update, force sources, stores and receivers of one
 // 4-cell group whose stress derivatives' raw parts are in hxx/hxz (row
 // windows) and zxz/zzz (z derivatives).
-template <typename T, bool PP>
+// OOP: the new velocities go to a.vx_o / a.vz_o (a step from one state
+// buffer into another); else in place.
+template <typename T, bool PP, bool OOP = false>
 __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const FusedExtras<T> &x, int tile,
                                                  int gi0, int gj, long long g, const Q4<T> &vxi,
                                                  const Q4<T> &vzi, const Q4<T> &r0, const Q4<T> &r1, T r4,
@@ -118,8 +120,8 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
     else
       add_lane4(vzn, k, a.dt * two_over_s(lane4(r0, k) + lane4(r1, k)) * f);
   }
-  stg4(a.vx + g, vxn);
-  stg4(a.vz + g, vzn);
+  stg4((OOP ? a.vx_o : a.vx) + g, vxn);
+  stg4((OOP ? a.vz_o : a.vz) + g, vzn);
   if (x.traces && x.it < x.tnt) {
     for (int e = e0; e < e1; ++e) {
       const int4 en = x.tile_ent[e];
@@ -131,8 +133,9 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
 }
 
 // PP: psi read from the input set and written to the output set (TTI);
-// else in place on the input set.
-template <typename T, bool PP>
+// else in place on the input set.  OOP (implies PP): v written to the
+// output state too.
+template <typename T, bool PP, bool OOP = false>
 __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                int tile) {
   using G = SplitGeom<T>;
@@ -172,7 +175,7 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
-  split_vel_finish<T, PP>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+  split_vel_finish<T, PP, OOP>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
 }
 
 // Tile height of the TMA-staged velocity pass (64 x 8: 34.8 Gpt/s on the
@@ -270,11 +273,11 @@ __global__ void __launch_bounds__(SplitVelTma<T>::NT, (sizeof(T) == 4 ? 1024 : 5
   split_vel_tma_tile<T, PP>(a, x, maps, blockIdx.x);
 }
 
-template <typename T, bool PP>
+template <typename T, bool PP, bool OOP>
 __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
     k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
   pdl_wait();  // the previous stress pass is complete and visible
-  split_vel_tile<T, PP>(a, x, blockIdx.x);
+  split_vel_tile<T, PP, OOP>(a, x, blockIdx.x);
 }
 
 // Batched: one tile of one shot per CTA; the step parity selects the shot's
@@ -291,7 +294,10 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
 }
 
 // ------------------------------------------------------------------ stress
-template <typename T, int KIND, int NSLS>
+// OOP: sigma, M and psi read from the input state and written to the
+// output one (a.sxx_o.., a.m_o, a.psix_o/psiz_o; the v maps then cover the
+// output velocities); else in place.
+template <typename T, int KIND, int NSLS, bool OOP = false>
 __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                   const SplitMaps &maps, int tile) {
   using G = SplitStressGeom<T>;
@@ -379,11 +385,13 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       if (xs >= 0) {
         const T *tb = a.tx;
         const long long o = (long long)gj * a.wx + xs;
-        T *p0 = a.psix + PX_VX * a.psix_plane + o, *p1 = a.psix + PX_VZ * a.psix_plane + o;
-        *p0 = tb[T_B * nx + gi] * *p0 + tb[T_A * nx + gi] * rxx.v[k];
-        *p1 = tb[T_BH * nx + gi] * *p1 + tb[T_AH * nx + gi] * dxvz.v[k];
-        rxx.v[k] = rxx.v[k] * tb[T_IK * nx + gi] + *p0;
-        dxvz.v[k] = dxvz.v[k] * tb[T_IKH * nx + gi] + *p1;
+        T *q = OOP ? a.psix_o : a.psix;
+        const T p0 = tb[T_B * nx + gi] * a.psix[PX_VX * a.psix_plane + o] + tb[T_A * nx + gi] * rxx.v[k];
+        const T p1 = tb[T_BH * nx + gi] * a.psix[PX_VZ * a.psix_plane + o] + tb[T_AH * nx + gi] * dxvz.v[k];
+        q[PX_VX * a.psix_plane + o] = p0;
+        q[PX_VZ * a.psix_plane + o] = p1;
+        rxx.v[k] = rxx.v[k] * tb[T_IK * nx + gi] + p0;
+        dxvz.v[k] = dxvz.v[k] * tb[T_IKH * nx + gi] + p1;
       }
     }
   }
@@ -392,11 +400,13 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const long long o = (long long)zs * nx + gi0 + k;
-      T *p0 = a.psiz + PZ_VZ * a.psiz_plane + o, *p1 = a.psiz + PZ_VX * a.psiz_plane + o;
-      *p0 = tb[T_B * nz + gj] * *p0 + tb[T_A * nz + gj] * rzz.v[k];
-      *p1 = tb[T_BH * nz + gj] * *p1 + tb[T_AH * nz + gj] * dzvx.v[k];
-      rzz.v[k] = rzz.v[k] * tb[T_IK * nz + gj] + *p0;
-      dzvx.v[k] = dzvx.v[k] * tb[T_IKH * nz + gj] + *p1;
+      T *q = OOP ? a.psiz_o : a.psiz;
+      const T p0 = tb[T_B * nz + gj] * a.psiz[PZ_VZ * a.psiz_plane + o] + tb[T_A * nz + gj] * rzz.v[k];
+      const T p1 = tb[T_BH * nz + gj] * a.psiz[PZ_VX * a.psiz_plane + o] + tb[T_AH * nz + gj] * dzvx.v[k];
+      q[PZ_VZ * a.psiz_plane + o] = p0;
+      q[PZ_VX * a.psiz_plane + o] = p1;
+      rzz.v[k] = rzz.v[k] * tb[T_IK * nz + gj] + p0;
+      dzvx.v[k] = dzvx.v[k] * tb[T_IKH * nz + gj] + p1;
     }
   }
   const Q4<T> rxz = add4(dzvx, dxvz);
@@ -438,7 +448,8 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       m[2 * NSLS + n] = fma4(dt4, fma4(a1, rxz, mul4(a2, m[2 * NSLS + n])), m[2 * NSLS + n]);
     }
 #pragma unroll
-    for (int q = 0; q < 3 * NSLS; ++q) stg4(a.m + q * a.mstride + g, m[q]);
+    for (int q = 0; q < 3 * NSLS; ++q)
+      stg4(OOP ? a.m_o + q * a.mstride_o + g : a.m + q * a.mstride + g, m[q]);
   }
   for (int e = e0; e < e1; ++e) {
     const int4 en = x.tile_ent[e];
@@ -448,9 +459,10 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
   }
   if (surf) szz = Q4<T>{{0, 0, 0, 0}};
-  stg4(a.sxx + g, sxx);
-  stg4(a.szz + g, szz);
-  stg4(a.sxz + g, sxz);
+  T *const osxx = OOP ? a.sxx_o : a.sxx, *const oszz = OOP ? a.szz_o : a.szz, *const osxz = OOP ? a.sxz_o : a.sxz;
+  stg4(osxx + g, sxx);
+  stg4(oszz + g, szz);
+  stg4(osxz + g, sxz);
   if (x.fs) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;
@@ -458,22 +470,22 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       Q4<T> im;
 #pragma unroll
       for (int q = 0; q < 4; ++q) im.v[q] = -szz.v[q];
-      stg4(a.szz + (long long)(L - k) * nx + gi0, im);
+      stg4(oszz + (long long)(L - k) * nx + gi0, im);
     }
     if (k >= 0 && k < L) {
       Q4<T> im;
 #pragma unroll
       for (int q = 0; q < 4; ++q) im.v[q] = -sxz.v[q];
-      stg4(a.sxz + (long long)(L - 1 - k) * nx + gi0, im);
+      stg4(osxz + (long long)(L - 1 - k) * nx + gi0, im);
     }
   }
 }
 
-template <typename T, int KIND, int NSLS>
+template <typename T, int KIND, int NSLS, bool OOP>
 __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                    const __grid_constant__ SplitMaps maps) {
-  split_stress_tile<T, KIND, NSLS>(a, x, maps, blockIdx.x);
+  split_stress_tile<T, KIND, NSLS, OOP>(a, x, maps, blockIdx.x);
 }
 
 template <typename T, int KIND, int NSLS>
@@ -487,32 +499,41 @@ __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 
 }
 
 // ------------------------------------------------------------------- host
-template <typename T, int KIND, int NSLS>
-static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
-                         int ntiles, cudaStream_t st, bool pdl) {
+template <typename T, int KIND, int NSLS, bool OOP>
+static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                           int ntiles, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS>, dim3(ntiles), dim3(SG::NT),
+  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP>, dim3(ntiles), dim3(SG::NT),
                                (size_t)SG::SMEM, st, pdl, a, x, m),
                     "split stress launch");
+}
+
+// out of place when the caller set the output state (a.sxx_o)
+template <typename T, int KIND, int NSLS>
+static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                         int ntiles, cudaStream_t st, bool pdl) {
+  return a.sxx_o ? launch_stress_k<T, KIND, NSLS, true>(a, x, m, ntiles, st, pdl)
+                 : launch_stress_k<T, KIND, NSLS, false>(a, x, m, ntiles, st, pdl);
 }
 
 template <typename T>
 int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, cudaStream_t st,
                      bool pdl) {
   using G = SplitGeom<T>;
-  const bool pp = a.psix_o != a.psix || a.psiz_o != a.psiz;
+  const bool oop = a.vx_o != nullptr, pp = oop || a.psix_o != a.psix || a.psiz_o != a.psiz;
   const cudaError_t e =
-      pp ? launch_pdl(k_split_vel_ldg<T, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
-         : launch_pdl(k_split_vel_ldg<T, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
+      oop  ? launch_pdl(k_split_vel_ldg<T, true, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+      : pp ? launch_pdl(k_split_vel_ldg<T, true, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+           : launch_pdl(k_split_vel_ldg<T, false, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
   return cuda_check(e, "split velocity launch");
 }
 
