@@ -33,6 +33,7 @@
 #include "plain.cuh"
 #include "plan.cuh"
 #include "split.cuh"
+#include "vec.cuh"
 
 namespace vb {
 
@@ -445,6 +446,84 @@ __global__ void k_div_t(AdjArgs<T> A, Slot<T> ab, const T *dbar) {
   }
 }
 
+// ---- 4-cell forms of the transposed derivatives (nx % 4 == 0, 16-byte
+// aligned planes): one thread per group of 4 x-adjacent cells, x taps from
+// a 12-value row window of three 128-bit loads, z taps as one 128-bit load
+// per row; per cell the same arithmetic as the scalar kernels.
+template <typename T>
+__device__ __forceinline__ void win12(const T *p, T (&o)[12]) {  // p[-4 .. +7]
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const Q4<T> v = ldc4(p - 4 + 4 * q);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[4 * q + k] = v.v[k];
+  }
+}
+template <typename T>
+__device__ __forceinline__ Q4<T> zp4(const T *p, long long s, const T *D) {  // ddzp form
+  Q4<T> acc = mul4(splat4<T>(D[0]), sub4(ldc4(p + s), ldc4(p)));
+#pragma unroll
+  for (int q = 1; q < 4; ++q) acc = fma4(splat4<T>(D[q]), sub4(ldc4(p + (q + 1) * s), ldc4(p - q * s)), acc);
+  return acc;
+}
+template <typename T>
+__device__ __forceinline__ Q4<T> zm4(const T *p, long long s, const T *D) {  // ddzm form
+  Q4<T> acc = mul4(splat4<T>(D[0]), sub4(ldc4(p), ldc4(p - s)));
+#pragma unroll
+  for (int q = 1; q < 4; ++q) acc = fma4(splat4<T>(D[q]), sub4(ldc4(p + q * s), ldc4(p - (q + 1) * s)), acc);
+  return acc;
+}
+
+// v += -D^T rbar, 4 cells per thread over the update region
+template <typename T>
+__global__ void __launch_bounds__(256) k_rates_t4(AdjArgs<T> A, Slot<T> ab, const T *rbar) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int gi0 = L + 4 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = L + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (gi0 >= A.nx - L || j >= A.nz - L) return;
+  const int nx = A.nx;
+  const long long g = (long long)j * nx + gi0, np = A.np;
+  T w0[12], w3[12];
+  win12(rbar + g, w0);
+  win12(rbar + 3 * np + g, w3);
+  const Q4<T> x0 = dps4(w0, A.Dx), x3 = dms4(w3, A.Dx);
+  const Q4<T> z2 = zm4(rbar + 2 * np + g, nx, A.Dz), z1 = zp4(rbar + np + g, nx, A.Dz);
+  const Q4<T> vx = ldc4(ab.vx() + g), vz = ldc4(ab.vz() + g);
+  stg4(ab.vx() + g, sub4(vx, add4(x0, z2)));
+  stg4(ab.vz() + g, sub4(vz, add4(z1, x3)));
+}
+
+// sigma += -D^T dbar, 4 cells per thread over every cell (groups whose taps
+// leave the planes take the checked scalar form)
+template <typename T>
+__global__ void __launch_bounds__(256) k_div_t4(AdjArgs<T> A, Slot<T> ab, const T *dbar) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int gi0 = 4 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int nx = A.nx, nz = A.nz;
+  if (gi0 >= nx || j >= nz) return;
+  const long long g = (long long)j * nx + gi0, np = A.np;
+  if (gi0 >= L && gi0 + 3 < nx - L && j >= L && j < nz - L) {
+    T w0[12], w2[12];
+    win12(dbar + g, w0);
+    win12(dbar + 2 * np + g, w2);
+    const Q4<T> sxx = ldc4(ab.sxx() + g), sxz = ldc4(ab.sxz() + g), szz = ldc4(ab.szz() + g);
+    stg4(ab.sxx() + g, sub4(sxx, dms4(w0, A.Dx)));
+    stg4(ab.sxz() + g, sub4(sxz, add4(zp4(dbar + np + g, nx, A.Dz), dps4(w2, A.Dx))));
+    stg4(ab.szz() + g, sub4(szz, zm4(dbar + 3 * np + g, nx, A.Dz)));
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = gi0 + k;
+      const long long c = g + k;
+      const T sxx = ab.sxx()[c], sxz = ab.sxz()[c], szz = ab.szz()[c];
+      ab.sxx()[c] = sxx - tap_m_b(dbar, i, j, nx, nz, 0, A.Dx);
+      ab.sxz()[c] = sxz - (tap_p_b(dbar + np, i, j, nx, nz, 1, A.Dz) + tap_p_b(dbar + 2 * np, i, j, nx, nz, 0, A.Dx));
+      ab.szz()[c] = szz - tap_m_b(dbar + 3 * np, i, j, nx, nz, 1, A.Dz);
+    }
+  }
+}
+
 // FP64 misfit: 1/2 sum (d - obs)^2 (one block, deterministic order)
 template <typename T>
 __global__ void k_misfit(const T *tr, const T *obs, long long n, double *out) {
@@ -689,6 +768,11 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   const dim3 blk(32, 8);
   const dim3 gU((c.nx - 2 * L + 31) / 32, (c.nz - 2 * L + 7) / 8);
   const dim3 gA((c.nx + 31) / 32, (c.nz + 7) / 8);
+  // 4-cell forms of the transposed derivatives where the planes allow
+  // 128-bit access (the same condition as the split pair)
+  const bool vec4 = use_split;
+  const dim3 gU4(((c.nx - 2 * L) / 4 + 31) / 32, (c.nz - 2 * L + 7) / 8);
+  const dim3 gA4((c.nx / 4 + 31) / 32, (c.nz + 7) / 8);
   int lrc = VI_OK;  // first launch error of the adjoint sweep
   auto lc = [&](auto kernel, dim3 g, dim3 b, auto... args) {
     const cudaError_t e = launch_pdl(kernel, g, b, 0, st, true, args...);
@@ -726,14 +810,20 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
         case 4: lc(k_stress_t<T, 4>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
         default: lc(k_stress_t<T, 5>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
       }
-      lc(k_rates_t<T>, gU, blk, A, ab, (const T *)rbar);
+      if (vec4)
+        lc(k_rates_t4<T>, gU4, blk, A, ab, (const T *)rbar);
+      else
+        lc(k_rates_t<T>, gU, blk, A, ab, (const T *)rbar);
       lc(k_residual<T>, dim3((nrec + 127) / 128), dim3(128), ab, x1, (const int2 *)p->drec, nrec, obs, nt, it, c.nx);
-      lc(k_vel_t<T>, gU, blk, A, x0, ab, rbar, h);
+      lc(k_vel_t<T>, gU, blk, A, x0, ab, rbar, h);  // the 4-cell form measured slower
       if (shot->nsrc > 0)
         lc(k_force_rho_t<T>, dim3((shot->nsrc + 127) / 128), dim3(128), A, ab, (const int4 *)p->dsrc,
            (const T *)p->damp, shot->nsrc, (const T *)shot->wavelet_dev, shot->wavelet_nt, it, h);
       lc(k_gather<T>, gA, blk, (const T *)h, gr, (const T *)q, g55, c.nx, c.nz);
-      lc(k_div_t<T>, gA, blk, A, ab, (const T *)rbar);
+      if (vec4)
+        lc(k_div_t4<T>, gA4, blk, A, ab, (const T *)rbar);
+      else
+        lc(k_div_t<T>, gA, blk, A, ab, (const T *)rbar);
     }
   }
   if (lrc) return lrc;

@@ -9,6 +9,7 @@
 // recomputation never reads a value another CTA has already advanced.
 // Per step each cell's state and medium cross HBM once: reads of v, sigma,
 // M, psi and the medium, writes of v, sigma, M and psi.
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <vector>
@@ -404,6 +405,9 @@ void build_tile_lists(int nx, int nz, int TX, int TZ, int HV, const vi_shot *s,
   off.assign(ntiles + 1, 0);
   ent.clear();
   for (int t = 0; t < ntiles; ++t) {
+    // by kind (force, explosive, receiver), in their original order within
+    // a kind: a loop over one kind stops at the first entry of the next
+    std::stable_sort(per[t].begin(), per[t].end(), [](const int4 &u, const int4 &v) { return u.w < v.w; });
     off[t] = (int)ent.size();
     ent.insert(ent.end(), per[t].begin(), per[t].end());
   }

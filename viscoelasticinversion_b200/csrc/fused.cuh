@@ -23,6 +23,7 @@ struct FusedGeom {
 };
 
 // tile-list entry kinds
+// entry kinds of the per-tile lists; a tile's entries are sorted by kind
 enum { TL_FORCE_X = 0, TL_FORCE_Z = 1, TL_EXPLOSIVE = 2, TL_RECEIVER = 3 };
 
 template <typename T>

@@ -108,10 +108,10 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
   Q4<T> vxn = fma4(mul4(dt4, bx), add4(dxx, zxz), vxi);
   Q4<T> vzn = fma4(mul4(dt4, bz), add4(dxxz, zzz), vzi);
   const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
-  for (int e = e0; e < e1; ++e) {  // force sources of this tile
+  for (int e = e0; e < e1; ++e) {  // force sources of this tile (listed first)
     const int4 en = x.tile_ent[e];
-    if ((en.w != TL_FORCE_X && en.w != TL_FORCE_Z) || en.y != gj || en.x < gi0 || en.x >= gi0 + 4)
-      continue;
+    if (en.w > TL_FORCE_Z) break;
+    if (en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
     const int k = en.x - gi0;
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
     const T f = x.amp[en.z] * w;
@@ -122,13 +122,25 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
   }
   stg4((OOP ? a.vx_o : a.vx) + g, vxn);
   stg4((OOP ? a.vz_o : a.vz) + g, vzn);
-  if (x.traces && x.it < x.tnt) {
-    for (int e = e0; e < e1; ++e) {
-      const int4 en = x.tile_ent[e];
-      if (en.w != TL_RECEIVER || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
-      x.traces[(long long)en.z * x.tnt + x.it] = lane4(vxn, en.x - gi0);
-      x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = lane4(vzn, en.x - gi0);
-    }
+}
+
+// Receivers of the tile, one thread per entry, read back from the tile's
+// new velocities after a barrier (every thread of the CTA calls it, after
+// the tile's stores): a tile on a receiver line then costs one load per
+// receiver instead of every thread scanning the whole list.
+template <typename T, bool OOP = false>
+__device__ __forceinline__ void split_vel_sample(const StepArgs<T> &a, const FusedExtras<T> &x, int tile) {
+  if (!x.traces || x.it >= x.tnt) return;
+  const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
+  if (e0 == e1) return;
+  __syncthreads();
+  const T *vx = OOP ? a.vx_o : a.vx, *vz = OOP ? a.vz_o : a.vz;
+  for (int e = e0 + (int)threadIdx.x; e < e1; e += (int)blockDim.x) {
+    const int4 en = x.tile_ent[e];
+    if (en.w != TL_RECEIVER) continue;
+    const long long c = (long long)en.y * a.nx + en.x;
+    x.traces[(long long)en.z * x.tnt + x.it] = vx[c];
+    x.traces[(long long)(x.nrec + en.z) * x.tnt + x.it] = vz[c];
   }
 }
 
@@ -271,6 +283,7 @@ __global__ void __launch_bounds__(SplitVelTma<T>::NT, (sizeof(T) == 4 ? 1024 : 5
     k_split_vel_tma(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
   pdl_wait();  // the previous stress pass is complete and visible
   split_vel_tma_tile<T, PP>(a, x, maps, blockIdx.x);
+  split_vel_sample<T>(a, x, blockIdx.x);
 }
 
 template <typename T, bool PP, bool OOP>
@@ -278,6 +291,7 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
     k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
   pdl_wait();  // the previous stress pass is complete and visible
   split_vel_tile<T, PP, OOP>(a, x, blockIdx.x);
+  split_vel_sample<T, OOP>(a, x, blockIdx.x);
 }
 
 // Batched: one tile of one shot per CTA; the step parity selects the shot's
@@ -291,6 +305,7 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
   split_vel_tile<T, PP>(b.args[2 * shot + (it & 1)], x, tile);
+  split_vel_sample<T>(b.args[2 * shot + (it & 1)], x, tile);
 }
 
 // ------------------------------------------------------------------ stress
@@ -451,9 +466,11 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     for (int q = 0; q < 3 * NSLS; ++q)
       stg4(OOP ? a.m_o + q * a.mstride_o + g : a.m + q * a.mstride + g, m[q]);
   }
-  for (int e = e0; e < e1; ++e) {
+  for (int e = e0; e < e1; ++e) {  // explosive sources (after the force ones, before receivers)
     const int4 en = x.tile_ent[e];
-    if (en.w != TL_EXPLOSIVE || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
+    if (en.w < TL_EXPLOSIVE) continue;
+    if (en.w > TL_EXPLOSIVE) break;
+    if (en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
     add_lane4(sxx, en.x - gi0, dt * x.amp[en.z] * w);
     add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);

@@ -266,9 +266,11 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
       stg4(a.m_o + (2 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxz, mul4(a2, mq)), mq));
     }
   }
-  for (int q = e0; q < e1; ++q) {
+  for (int q = e0; q < e1; ++q) {  // explosive sources (after the force ones, before receivers)
     const int4 en = x.tile_ent[q];
-    if (en.w != TL_EXPLOSIVE || en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
+    if (en.w < TL_EXPLOSIVE) continue;
+    if (en.w > TL_EXPLOSIVE) break;
+    if (en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
     add_lane4(sxx, en.x - gi0, dt * x.amp[en.z] * w);
     add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
