@@ -229,7 +229,7 @@ def measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=False):
     b.run()  # tunes the kernel form, captures the graph, runs once
     b.reset()
     form = b.status()
-    variant = {"split": 5, "two-stage": 3, "one-stage": 4}[form]
+    variant = {"per-shot": 0, "split": 5, "two-stage": 3, "one-stage": 4}[form]
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -10,9 +10,11 @@
 // order and a launch covers items [0, prefix[active]).
 //
 // Kernel forms: the TMA-staged fused step (one launch per time step; two-
-// stage persistent tiles or one-stage tiles) or the split pair (a velocity
+// stage persistent tiles or one-stage tiles), the split pair (a velocity
 // and a stress launch per time step, in place; TTI memory variables and
-// psi ping-pong by step parity).  The autotuner picks the form by timing a
+// psi ping-pong by step parity), or per shot (each shot's own vi_step time
+// loop, one shot after the other: the fastest when every shot fills the
+// GPU by itself).  The autotuner picks the form by timing a
 // few steps of each on the bound shots and caches the choice per (medium,
 // precision, mechanisms, grid set).
 #include <algorithm>
@@ -53,7 +55,7 @@ struct vi_batch {
 
 namespace vb {
 
-constexpr int kFormOneStage = 0, kFormTwoStage = 1, kFormSplit = 2;
+constexpr int kFormOneStage = 0, kFormTwoStage = 1, kFormSplit = 2, kFormPerShot = 3;
 
 static std::map<std::string, int> g_tuned;  // kernel form chosen per problem class
 
@@ -66,6 +68,15 @@ static std::string tune_key(const vi_batch *b) {
                   std::to_string(b->nsls);
   for (auto &p : g) k += "/" + std::to_string(p.first) + "x" + std::to_string(p.second);
   return k;
+}
+
+// Processing order (descending step count, so the shots active at step it
+// form a prefix) and the longest step count.
+static void set_order(vi_batch *b) {
+  b->order.resize(b->n);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->nt[x] > b->nt[y]; });
+  b->max_nt = b->n ? b->nt[b->order[0]] : 0;
 }
 
 // Builds every per-shot device structure for one kernel form and uploads it.
@@ -173,21 +184,22 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
     x.err = b->err;
   }
   // descending step count: the shots active at step it form a prefix
-  b->order.resize(n);
-  std::iota(b->order.begin(), b->order.end(), 0);
-  std::stable_sort(b->order.begin(), b->order.end(),
-                   [&](int x, int y) { return b->nt[x] > b->nt[y]; });
+  set_order(b);
   b->prefix.assign(n + 1, 0);
   for (int q = 0; q < n; ++q) b->prefix[q + 1] = b->prefix[q] + ntiles[b->order[q]];
-  b->max_nt = n ? b->nt[b->order[0]] : 0;
-  // one device block: args | ext | maps | smaps | prefix | order
+  // (shot, tile) of every item, so a CTA finds its tile with one load
+  std::vector<int2> items((size_t)b->prefix[n]);
+  for (int q = 0; q < n; ++q)
+    for (int t = 0; t < ntiles[b->order[q]]; ++t) items[(size_t)b->prefix[q] + t] = make_int2(b->order[q], t);
+  // one device block: args | ext | maps | smaps | prefix | order | items
   auto up = [](size_t x) { return (x + 127) / 128 * 128; };
   const size_t o_args = 0, o_ext = up(o_args + args.size() * sizeof(StepArgs<T>));
   const size_t o_maps = up(o_ext + ext.size() * sizeof(FusedExtras<T>));
   const size_t o_smaps = up(o_maps + maps.size() * sizeof(TmaMaps));
   const size_t o_pre = up(o_smaps + smaps.size() * sizeof(SplitMaps));
   const size_t o_ord = up(o_pre + b->prefix.size() * sizeof(int));
-  const size_t total = up(o_ord + b->order.size() * sizeof(int));
+  const size_t o_items = up(o_ord + b->order.size() * sizeof(int));
+  const size_t total = up(o_items + items.size() * sizeof(int2));
   if (b->dev_bytes < total) {
     if (b->dev) cudaFree(b->dev);
     b->dev = nullptr;
@@ -205,6 +217,7 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
   std::memcpy(host.data() + o_smaps, smaps.data(), smaps.size() * sizeof(SplitMaps));
   std::memcpy(host.data() + o_pre, b->prefix.data(), b->prefix.size() * sizeof(int));
   std::memcpy(host.data() + o_ord, b->order.data(), b->order.size() * sizeof(int));
+  std::memcpy(host.data() + o_items, items.data(), items.size() * sizeof(int2));
   if ((rc = cuda_check(cudaMemcpyAsync(b->dev, host.data(), total, cudaMemcpyHostToDevice, st),
                        "upload batch table")))
     return rc;
@@ -216,6 +229,7 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
   bd.smaps = (const SplitMaps *)(d + o_smaps);
   bd.prefix = (const int *)(d + o_pre);
   bd.order = (const int *)(d + o_ord);
+  bd.items = (const int2 *)(d + o_items);
   bd.nshots = n;
   bd.err = b->err;
   return VI_OK;
@@ -268,6 +282,47 @@ static int reset_state(vi_batch *b, cudaStream_t st) {
   return VI_OK;
 }
 
+
+// The per-shot form: steps [it0, it1) of every shot (capped at its step
+// count) through vi_step, one shot after the other.
+static int per_shot_steps(vi_batch *b, int it0, int it1, cudaStream_t st) {
+  for (int q = 0; q < b->n; ++q) {
+    const int i = b->order[q];
+    const int n = std::min(it1, b->nt[i]) - it0;
+    if (n <= 0) continue;
+    const int rc = vi_step(b->plans[i], &b->med[i], &b->fields[i], &b->shot[i], it0, n, 0, st);
+    if (rc) return rc;
+  }
+  return VI_OK;
+}
+
+// Marginal time of 8 more steps of every shot for one form (the time of
+// 16 steps minus that of 8), so one-time costs per call — host staging of
+// the per-shot form — do not decide between forms.
+template <typename F>
+static int time_marginal(F run_steps, cudaStream_t st, int max_nt, float *ms) {
+  const int s1 = std::min(8, max_nt), s2 = std::min(16, max_nt);
+  int rc = run_steps(0, 2);  // warm-up
+  if (rc) return rc;
+  float t[2] = {0, 0};
+  const int n[2] = {s1, s2};
+  for (int k = 0; k < 2; ++k) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    rc = run_steps(0, n[k]);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&t[k], e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+  }
+  *ms = s2 > s1 ? t[1] - t[0] : t[1];
+  return VI_OK;
+}
+
 template <typename T>
 static int tune(vi_batch *b, cudaStream_t st) {
   const std::string key = tune_key(b);
@@ -276,30 +331,25 @@ static int tune(vi_batch *b, cudaStream_t st) {
     b->form = hit->second;
     return VI_OK;
   }
+  set_order(b);
   float best = 1e30f;
   int choice = kFormTwoStage;
   // double precision has one fused form (two stages do not fit)
-  const int forms[3] = {kFormSplit, kFormTwoStage, kFormOneStage};
-  const int nforms = sizeof(T) == 4 ? 3 : 2;
+  const int forms[4] = {kFormPerShot, kFormSplit, kFormTwoStage, kFormOneStage};
+  const int nforms = sizeof(T) == 4 ? 4 : 3;
   for (int f = 0; f < nforms; ++f) {
     const int form = forms[f];
-    BatchDev<T> bd;
-    int rc = prepare<T>(b, form, st, bd);
-    if (rc == VI_ERR_ARG) continue;
-    if (rc) return rc;
-    const int steps = std::min(8, b->max_nt);
-    if ((rc = launch_steps<T>(b, bd, form, 0, 2, st))) return rc;  // warm-up
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
-    rc = launch_steps<T>(b, bd, form, 0, steps, st);
-    cudaEventRecord(e1, st);
-    cudaEventSynchronize(e1);
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    int rc;
+    if (form == kFormPerShot) {
+      rc = time_marginal([&](int a, int e) { return per_shot_steps(b, a, e, st); }, st, b->max_nt, &ms);
+    } else {
+      BatchDev<T> bd;
+      rc = prepare<T>(b, form, st, bd);
+      if (rc == VI_ERR_ARG) continue;
+      if (rc) return rc;
+      rc = time_marginal([&](int a, int e) { return launch_steps<T>(b, bd, form, a, e, st); }, st, b->max_nt, &ms);
+    }
     if (rc) return rc;
     if (ms < best) {
       best = ms;
@@ -334,6 +384,12 @@ static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
   const int form = b->form;
   for (int i = 0; i < b->n; ++i)
     if ((rc = vi_plan_reset(b->plans[i], st))) return rc;
+  if (form == kFormPerShot) {
+    set_order(b);
+    for (int i = 0; i < b->n; ++i) b->plans[i]->psi_cur = 0;
+    if ((rc = per_shot_steps(b, 0, b->max_nt, st))) return rc;
+    return cuda_check(cudaGetLastError(), "batch run");
+  }
   if (b->dirty || !use_graph || b->graph_form != form) {
     BatchDev<T> bd;
     if ((rc = prepare<T>(b, form, st, bd))) return rc;

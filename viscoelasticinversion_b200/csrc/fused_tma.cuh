@@ -113,15 +113,23 @@ struct BatchDev {
   const SplitMaps *smaps;     // [nshots] (split kernel form)
   const int *prefix;          // [nshots + 1] tile offsets in processing order
   const int *order;           // [nshots] shot at each processing position
+  const int2 *items;          // [prefix[nshots]] (shot, tile) of every item
   int nshots;
   int *err;
 };
 
 #ifdef __CUDACC__
 // The shot and tile of batch item `item` (items are the tiles of the shots
-// in processing order): the largest position p with prefix[p] <= item.
+// in processing order): from the item table, else by binary search for the
+// largest position p with prefix[p] <= item.
 template <typename T>
 __device__ __forceinline__ void batch_locate(const BatchDev<T> &b, int item, int &shot, int &tile) {
+  if (b.items) {  // one load instead of a chain of dependent ones
+    const int2 v = b.items[item];
+    shot = v.x;
+    tile = v.y;
+    return;
+  }
   int lo = 0, hi = b.nshots - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;

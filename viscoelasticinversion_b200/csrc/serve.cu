@@ -128,7 +128,10 @@ struct vi_server {
 
 namespace {
 
-constexpr size_t kPlanCache = 8;
+// up to 64 plans and 16 GB of plan workspace are kept; beyond that the
+// oldest is destroyed (a device-wide free)
+constexpr size_t kPlanCache = 64;
+constexpr size_t kPlanCacheBytes = 16ull << 30;
 
 bool same_config(const vi_config &a, const vi_config &b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
 
@@ -150,16 +153,19 @@ int take_plan(vi_server *s, const vi_config &c, vi_plan **out) {
 
 // Keeps a finished request's plan for reuse (oldest evicted beyond the cap).
 void give_plan(vi_server *s, vi_plan *p) {
-  vi_plan *evict = nullptr;
+  std::vector<vi_plan *> evict;
   {
     std::lock_guard<std::mutex> lk(s->plan_mu);
     s->plan_cache.push_back(p);
-    if (s->plan_cache.size() > kPlanCache) {
-      evict = s->plan_cache.front();
+    size_t bytes = 0;
+    for (vi_plan *c : s->plan_cache) bytes += c->bytes;
+    while (s->plan_cache.size() > 1 && (s->plan_cache.size() > kPlanCache || bytes > kPlanCacheBytes)) {
+      bytes -= s->plan_cache.front()->bytes;
+      evict.push_back(s->plan_cache.front());
       s->plan_cache.erase(s->plan_cache.begin());
     }
   }
-  if (evict) vi_plan_destroy(evict);
+  for (vi_plan *c : evict) vi_plan_destroy(c);
 }
 
 template <typename T>
