@@ -120,8 +120,9 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
     else
       add_lane4(vzn, k, a.dt * two_over_s(lane4(r0, k) + lane4(r1, k)) * f);
   }
-  stg4((OOP ? a.vx_o : a.vx) + g, vxn);
-  stg4((OOP ? a.vz_o : a.vz) + g, vzn);
+  // v is re-read by the stress pass of the same step: keep it in L2
+  sth4((OOP ? a.vx_o : a.vx) + g, vxn, l2_keep());
+  sth4((OOP ? a.vz_o : a.vz) + g, vzn, l2_keep());
 }
 
 // Receivers of the tile, one thread per entry, read back from the tile's
@@ -344,19 +345,19 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     sxx = ldc4(a.sxx + g);
     szz = ldc4(a.szz + g);
     sxz = ldc4(a.sxz + g);
-    c13 = ldg4(a.c13 + g);
+    c13 = ldgh4(a.c13 + g, l2_stream());
     c55a = ldg4(a.c55 + g);
     c55b = ldg4(a.c55 + g + nx);
     c55a4 = __ldg(a.c55 + g + 4);
     c55b4 = __ldg(a.c55 + g + nx + 4);
     if constexpr (KIND != VI_MEDIUM_ISO) {
-      c11 = ldg4(a.c11 + g);
-      c33 = ldg4(a.c33 + g);
+      c11 = ldgh4(a.c11 + g, l2_stream());
+      c33 = ldgh4(a.c33 + g, l2_stream());
     }
     if constexpr (NSLS > 0) {
-      tau = ldg4(a.tau + g);
+      tau = ldgh4(a.tau + g, l2_stream());
 #pragma unroll
-      for (int q = 0; q < 3 * NSLS; ++q) m[q] = ldc4(a.m + q * a.mstride + g);
+      for (int q = 0; q < 3 * NSLS; ++q) m[q] = ldh4(a.m + q * a.mstride + g, l2_stream());
     }
   }
   const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
@@ -464,7 +465,7 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     }
 #pragma unroll
     for (int q = 0; q < 3 * NSLS; ++q)
-      stg4(OOP ? a.m_o + q * a.mstride_o + g : a.m + q * a.mstride + g, m[q]);
+      sth4(OOP ? a.m_o + q * a.mstride_o + g : a.m + q * a.mstride + g, m[q], l2_stream());
   }
   for (int e = e0; e < e1; ++e) {  // explosive sources (after the force ones, before receivers)
     const int4 en = x.tile_ent[e];
@@ -477,9 +478,10 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   }
   if (surf) szz = Q4<T>{{0, 0, 0, 0}};
   T *const osxx = OOP ? a.sxx_o : a.sxx, *const oszz = OOP ? a.szz_o : a.szz, *const osxz = OOP ? a.sxz_o : a.sxz;
-  stg4(osxx + g, sxx);
-  stg4(oszz + g, szz);
-  stg4(osxz + g, sxz);
+  // sigma is re-read by the next velocity pass: keep it in L2
+  sth4(osxx + g, sxx, l2_keep());
+  sth4(oszz + g, szz, l2_keep());
+  sth4(osxz + g, sxz, l2_keep());
   if (x.fs) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;

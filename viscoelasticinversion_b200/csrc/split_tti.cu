@@ -231,7 +231,9 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   const Q4<T> dt4 = splat4<T>(dt);
   const bool surf = x.fs && gj == L;
   Q4<T> sxx = ldc4(a.sxx + g), szz = ldc4(a.szz + g), sxz = ldc4(a.sxz + g);
-  const Q4<T> C11 = ldg4(a.c11 + g), C13 = ldg4(a.c13 + g), C33 = ldg4(a.c33 + g);
+  // read once per step: streamed through L2 (ring-shared operands are not)
+  const Q4<T> C11 = ldgh4(a.c11 + g, l2_stream()), C13 = ldgh4(a.c13 + g, l2_stream()),
+              C33 = ldgh4(a.c33 + g, l2_stream());
   const Q4<T> c15a = ldg4(a.c15 + g), c15b = ldg4(a.c15 + g + nx);
   const Q4<T> c35a = ldg4(a.c35 + g), c35b = ldg4(a.c35 + g + nx);
   const Q4<T> c55a = ldg4(a.c55 + g), c55b = ldg4(a.c55 + g + nx);
@@ -260,10 +262,10 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
       const Q4<T> mx = ldc4(a.m + (0 * NSLS + n) * a.mstride + g);
       const Q4<T> mz = ldc4(a.m + (1 * NSLS + n) * a.mstride + g);
       const Q4<T> mq = ldc4(a.m + (2 * NSLS + n) * a.mstride + g);
-      stg4(a.m_o + (0 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxx, mul4(a2, mx)), mx));
-      stg4(a.m_o + (1 * NSLS + n) * a.mstride_o + g,
-           surf ? splat4<T>(0) : fma4(dt4, fma4(a1, rzz, mul4(a2, mz)), mz));
-      stg4(a.m_o + (2 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxz, mul4(a2, mq)), mq));
+      sth4(a.m_o + (0 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxx, mul4(a2, mx)), mx), l2_stream());
+      sth4(a.m_o + (1 * NSLS + n) * a.mstride_o + g,
+           surf ? splat4<T>(0) : fma4(dt4, fma4(a1, rzz, mul4(a2, mz)), mz), l2_stream());
+      sth4(a.m_o + (2 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxz, mul4(a2, mq)), mq), l2_stream());
     }
   }
   for (int q = e0; q < e1; ++q) {  // explosive sources (after the force ones, before receivers)
@@ -276,9 +278,10 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
     add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
   }
   if (surf) szz = splat4<T>(0);
-  stg4(a.sxx + g, sxx);
-  stg4(a.szz + g, szz);
-  stg4(a.sxz + g, sxz);
+  // sigma is re-read by the next velocity pass: keep it in L2
+  sth4(a.sxx + g, sxx, l2_keep());
+  sth4(a.szz + g, szz, l2_keep());
+  sth4(a.sxz + g, sxz, l2_keep());
   if (x.fs) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;

@@ -3,6 +3,8 @@
 // on multiples of 4 elements, so every vector access is 16-byte aligned.
 #pragma once
 
+#include <cstdint>
+
 #include <cuda_runtime.h>
 
 namespace vb {
@@ -53,6 +55,56 @@ __device__ __forceinline__ void add_lane4(Q4<T> &q, int k, T d) {
 #pragma unroll
   for (int i = 0; i < 4; ++i)
     if (i == k) q.v[i] += d;
+}
+// ---- L2 eviction priority hints (createpolicy + .L2::cache_hint): lines
+// re-read by the other pass of the step are kept (evict_last), lines that
+// are read or written once per step go first (evict_first)
+__device__ __forceinline__ uint64_t l2_keep() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_stream() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void sth4(float *p, const Q4<float> &q, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(q.v[0]), "f"(q.v[1]),
+               "f"(q.v[2]), "f"(q.v[3]), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void sth4(double *p, const Q4<double> &q, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(q.v[0]), "d"(q.v[1]), "l"(pol)
+               : "memory");
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p + 2), "d"(q.v[2]), "d"(q.v[3]), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ Q4<float> ldh4(const float *p, uint64_t pol) {
+  Q4<float> q;
+  asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(q.v[0]), "=f"(q.v[1]), "=f"(q.v[2]), "=f"(q.v[3])
+               : "l"(p), "l"(pol));
+  return q;
+}
+__device__ __forceinline__ Q4<double> ldh4(const double *p, uint64_t pol) {
+  Q4<double> q;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[0]), "=d"(q.v[1]) : "l"(p), "l"(pol));
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[2]), "=d"(q.v[3]) : "l"(p + 2), "l"(pol));
+  return q;
+}
+__device__ __forceinline__ Q4<float> ldgh4(const float *p, uint64_t pol) {  // read-only data
+  Q4<float> q;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(q.v[0]), "=f"(q.v[1]), "=f"(q.v[2]), "=f"(q.v[3])
+               : "l"(p), "l"(pol));
+  return q;
+}
+__device__ __forceinline__ Q4<double> ldgh4(const double *p, uint64_t pol) {
+  Q4<double> q;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[0]), "=d"(q.v[1]) : "l"(p), "l"(pol));
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[2]), "=d"(q.v[3]) : "l"(p + 2), "l"(pol));
+  return q;
 }
 __device__ __forceinline__ void stg4(float *p, const Q4<float> &q) {
   *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
