@@ -687,6 +687,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     fx.nrec = nrec;
     fx.tnt = nt;
     fx.err = (int *)p->errflag;
+    fx.l2hint = l2_hints_fit(5LL * c.nx * c.nz * (long long)sizeof(T), p->l2_bytes);
     const int sntx_keep = fxs.ntx;
     const int *soff_keep = fxs.tile_off;
     fxs = fx;

@@ -95,6 +95,8 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
   std::vector<TmaMaps> maps(split ? 0 : 2 * n);
   std::vector<SplitMaps> smaps(split ? n : 0);
   std::vector<int> ntiles(n);
+  long long kept = 0;  // planes the split kernels keep in L2, over every shot
+  for (int i = 0; i < n; ++i) kept += 5LL * b->plans[i]->cfg.nx * b->plans[i]->cfg.nz * (long long)sizeof(T);
   int rc;
   for (int i = 0; i < n; ++i) {
     vi_plan *p = b->plans[i];
@@ -182,6 +184,7 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
     x.tnt = sh.nrec ? sh.traces_nt : 0;
     x.nrec = sh.nrec;
     x.err = b->err;
+    x.l2hint = l2_hints_fit(kept, p->l2_bytes);
   }
   // descending step count: the shots active at step it form a prefix
   set_order(b);

@@ -364,6 +364,11 @@ extern "C" int vi_plan_create(const vi_config *cfg, vi_plan **out) {
   vi_plan *p = new vi_plan();
   p->cfg = *cfg;
   cudaGetDevice(&p->device);
+  int l2 = 0;
+  if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, p->device) == cudaSuccess && l2 > 0)
+    p->l2_bytes = l2;
+  else
+    cudaGetLastError();
   if (cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess ||
       p->nsm <= 0) {
     cudaGetLastError();

@@ -39,6 +39,7 @@ struct FusedExtras {
   T *traces;
   int tnt, nrec;
   int *err;                // device error word (bounded waits that gave up)
+  int l2hint;              // split kernels: L2 eviction priorities (see vec.cuh)
 };
 
 // Runs nsteps fused steps, ping-ponging between the caller's fields (in

@@ -10,6 +10,7 @@ struct vi_plan {
   vi_config cfg;
   int device = 0;
   int nsm = 148;  // streaming multiprocessors of the device
+  long long l2_bytes = 126ll << 20;  // L2 cache of the device
   int Lx = 0, Rx = 0, Tz = 0, Bz = 0, wx = 0, hz = 0;
   size_t esize = 4;  // bytes per real
   // device workspace
@@ -45,6 +46,9 @@ int ensure_buffer(vi_plan *p, void **buf, size_t *have, size_t need);
 template <typename T>
 StepArgs<T> make_args(const vi_plan *p, const vi_medium *m, const vi_fields *f);
 int check_medium(const vi_plan *p, const vi_medium *m);
+// Whether the split kernels' L2 eviction priorities pay off: the planes
+// they keep (the new v and sigma, 5 per shot) fit in half the L2.
+inline bool l2_hints_fit(long long kept_bytes, long long l2_bytes) { return 2 * kept_bytes <= l2_bytes; }
 int check_fields(const vi_plan *p, const vi_fields *f);
 // Copies a shot's source / receiver lists to the plan's device buffers.
 template <typename T>

@@ -57,7 +57,7 @@ namespace vb {
 // windows) and zxz/zzz (z derivatives).
 // OOP: the new velocities go to a.vx_o / a.vz_o (a step from one state
 // buffer into another); else in place.
-template <typename T, bool PP, bool OOP = false>
+template <typename T, bool PP, bool OOP, bool HINT>
 __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const FusedExtras<T> &x, int tile,
                                                  int gi0, int gj, long long g, const Q4<T> &vxi,
                                                  const Q4<T> &vzi, const Q4<T> &r0, const Q4<T> &r1, T r4,
@@ -121,8 +121,8 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
       add_lane4(vzn, k, a.dt * two_over_s(lane4(r0, k) + lane4(r1, k)) * f);
   }
   // v is re-read by the stress pass of the same step: keep it in L2
-  sth4((OOP ? a.vx_o : a.vx) + g, vxn, l2_keep());
-  sth4((OOP ? a.vz_o : a.vz) + g, vzn, l2_keep());
+  sth4((OOP ? a.vx_o : a.vx) + g, vxn, l2_keep_c<HINT>());
+  sth4((OOP ? a.vz_o : a.vz) + g, vzn, l2_keep_c<HINT>());
 }
 
 // Receivers of the tile, one thread per entry, read back from the tile's
@@ -148,7 +148,7 @@ __device__ __forceinline__ void split_vel_sample(const StepArgs<T> &a, const Fus
 // PP: psi read from the input set and written to the output set (TTI);
 // else in place on the input set.  OOP (implies PP): v written to the
 // output state too.
-template <typename T, bool PP, bool OOP = false>
+template <typename T, bool PP, bool OOP, bool HINT>
 __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                int tile) {
   using G = SplitGeom<T>;
@@ -188,7 +188,7 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
-  split_vel_finish<T, PP, OOP>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+  split_vel_finish<T, PP, OOP, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
 }
 
 // Tile height of the TMA-staged velocity pass (64 x 8: 34.8 Gpt/s on the
@@ -215,7 +215,7 @@ struct SplitVelTma {
   static_assert((WX * TZ * sizeof(T)) % 16 == 0 && (WX * HZ * sizeof(T)) % 16 == 0, "16-byte boxes");
 };
 
-template <typename T, bool PP>
+template <typename T, bool PP, bool HINT>
 __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                    const SplitMaps &maps, int tile) {
   using G = SplitVelTma<T>;
@@ -276,22 +276,22 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
-  split_vel_finish<T, PP>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+  split_vel_finish<T, PP, false, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
 }
 
-template <typename T, bool PP>
+template <typename T, bool PP, bool HINT>
 __global__ void __launch_bounds__(SplitVelTma<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitVelTma<T>::NT)
     k_split_vel_tma(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
   pdl_wait();  // the previous stress pass is complete and visible
-  split_vel_tma_tile<T, PP>(a, x, maps, blockIdx.x);
+  split_vel_tma_tile<T, PP, HINT>(a, x, maps, blockIdx.x);
   split_vel_sample<T>(a, x, blockIdx.x);
 }
 
-template <typename T, bool PP, bool OOP>
+template <typename T, bool PP, bool OOP, bool HINT>
 __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
     k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
   pdl_wait();  // the previous stress pass is complete and visible
-  split_vel_tile<T, PP, OOP>(a, x, blockIdx.x);
+  split_vel_tile<T, PP, OOP, HINT>(a, x, blockIdx.x);
   split_vel_sample<T, OOP>(a, x, blockIdx.x);
 }
 
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  split_vel_tile<T, PP>(b.args[2 * shot + (it & 1)], x, tile);
+  split_vel_tile<T, PP, false, false>(b.args[2 * shot + (it & 1)], x, tile);
   split_vel_sample<T>(b.args[2 * shot + (it & 1)], x, tile);
 }
 
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
 // OOP: sigma, M and psi read from the input state and written to the
 // output one (a.sxx_o.., a.m_o, a.psix_o/psiz_o; the v maps then cover the
 // output velocities); else in place.
-template <typename T, int KIND, int NSLS, bool OOP = false>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT>
 __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                   const SplitMaps &maps, int tile) {
   using G = SplitStressGeom<T>;
@@ -345,19 +345,19 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     sxx = ldc4(a.sxx + g);
     szz = ldc4(a.szz + g);
     sxz = ldc4(a.sxz + g);
-    c13 = ldgh4(a.c13 + g, l2_stream());
+    c13 = ldgh4(a.c13 + g, l2_stream_c<HINT>());
     c55a = ldg4(a.c55 + g);
     c55b = ldg4(a.c55 + g + nx);
     c55a4 = __ldg(a.c55 + g + 4);
     c55b4 = __ldg(a.c55 + g + nx + 4);
     if constexpr (KIND != VI_MEDIUM_ISO) {
-      c11 = ldgh4(a.c11 + g, l2_stream());
-      c33 = ldgh4(a.c33 + g, l2_stream());
+      c11 = ldgh4(a.c11 + g, l2_stream_c<HINT>());
+      c33 = ldgh4(a.c33 + g, l2_stream_c<HINT>());
     }
     if constexpr (NSLS > 0) {
-      tau = ldgh4(a.tau + g, l2_stream());
+      tau = ldgh4(a.tau + g, l2_stream_c<HINT>());
 #pragma unroll
-      for (int q = 0; q < 3 * NSLS; ++q) m[q] = ldh4(a.m + q * a.mstride + g, l2_stream());
+      for (int q = 0; q < 3 * NSLS; ++q) m[q] = ldh4(a.m + q * a.mstride + g, l2_stream_c<HINT>());
     }
   }
   const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
@@ -465,7 +465,7 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     }
 #pragma unroll
     for (int q = 0; q < 3 * NSLS; ++q)
-      sth4(OOP ? a.m_o + q * a.mstride_o + g : a.m + q * a.mstride + g, m[q], l2_stream());
+      sth4(OOP ? a.m_o + q * a.mstride_o + g : a.m + q * a.mstride + g, m[q], l2_stream_c<HINT>());
   }
   for (int e = e0; e < e1; ++e) {  // explosive sources (after the force ones, before receivers)
     const int4 en = x.tile_ent[e];
@@ -479,9 +479,9 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   if (surf) szz = Q4<T>{{0, 0, 0, 0}};
   T *const osxx = OOP ? a.sxx_o : a.sxx, *const oszz = OOP ? a.szz_o : a.szz, *const osxz = OOP ? a.sxz_o : a.sxz;
   // sigma is re-read by the next velocity pass: keep it in L2
-  sth4(osxx + g, sxx, l2_keep());
-  sth4(oszz + g, szz, l2_keep());
-  sth4(osxz + g, sxz, l2_keep());
+  sth4(osxx + g, sxx, l2_keep_c<HINT>());
+  sth4(oszz + g, szz, l2_keep_c<HINT>());
+  sth4(osxz + g, sxz, l2_keep_c<HINT>());
   if (x.fs) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;
@@ -500,11 +500,11 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   }
 }
 
-template <typename T, int KIND, int NSLS, bool OOP>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT>
 __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                    const __grid_constant__ SplitMaps maps) {
-  split_stress_tile<T, KIND, NSLS, OOP>(a, x, maps, blockIdx.x);
+  split_stress_tile<T, KIND, NSLS, OOP, HINT>(a, x, maps, blockIdx.x);
 }
 
 template <typename T, int KIND, int NSLS>
@@ -514,11 +514,11 @@ __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  split_stress_tile<T, KIND, NSLS>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  split_stress_tile<T, KIND, NSLS, false, false>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
 // ------------------------------------------------------------------- host
-template <typename T, int KIND, int NSLS, bool OOP>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT>
 static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                            int ntiles, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
@@ -526,12 +526,12 @@ static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const 
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP, HINT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP>, dim3(ntiles), dim3(SG::NT),
+  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP, HINT>, dim3(ntiles), dim3(SG::NT),
                                (size_t)SG::SMEM, st, pdl, a, x, m),
                     "split stress launch");
 }
@@ -540,8 +540,10 @@ static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const 
 template <typename T, int KIND, int NSLS>
 static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                          int ntiles, cudaStream_t st, bool pdl) {
-  return a.sxx_o ? launch_stress_k<T, KIND, NSLS, true>(a, x, m, ntiles, st, pdl)
-                 : launch_stress_k<T, KIND, NSLS, false>(a, x, m, ntiles, st, pdl);
+  // the out-of-place form (the gradient's recompute) always hints
+  if (a.sxx_o) return launch_stress_k<T, KIND, NSLS, true, true>(a, x, m, ntiles, st, pdl);
+  return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true>(a, x, m, ntiles, st, pdl)
+                  : launch_stress_k<T, KIND, NSLS, false, false>(a, x, m, ntiles, st, pdl);
 }
 
 template <typename T>
@@ -550,9 +552,11 @@ int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, 
   using G = SplitGeom<T>;
   const bool oop = a.vx_o != nullptr, pp = oop || a.psix_o != a.psix || a.psiz_o != a.psiz;
   const cudaError_t e =
-      oop  ? launch_pdl(k_split_vel_ldg<T, true, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
-      : pp ? launch_pdl(k_split_vel_ldg<T, true, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
-           : launch_pdl(k_split_vel_ldg<T, false, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
+      oop         ? launch_pdl(k_split_vel_ldg<T, true, true, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+      : pp        ? (x.l2hint ? launch_pdl(k_split_vel_ldg<T, true, false, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+                              : launch_pdl(k_split_vel_ldg<T, true, false, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x))
+      : x.l2hint  ? launch_pdl(k_split_vel_ldg<T, false, false, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+                  : launch_pdl(k_split_vel_ldg<T, false, false, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
   return cuda_check(e, "split velocity launch");
 }
 
@@ -637,15 +641,18 @@ static int launch_vel_tma(const StepArgs<T> &a, const FusedExtras<T> &x, const S
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    for (auto k : {k_split_vel_tma<T, true>, k_split_vel_tma<T, false>}) {
+    for (auto k : {k_split_vel_tma<T, true, true>, k_split_vel_tma<T, false, true>, k_split_vel_tma<T, true, false>,
+                   k_split_vel_tma<T, false, false>}) {
       const cudaError_t ea = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
       if (ea != cudaSuccess) return cuda_check(ea, "split velocity (TMA) smem attribute");
     }
     attr_set |= 1ULL << dev;
   }
   const cudaError_t e =
-      pp ? launch_pdl(k_split_vel_tma<T, true>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
-         : launch_pdl(k_split_vel_tma<T, false>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m);
+      pp ? (x.l2hint ? launch_pdl(k_split_vel_tma<T, true, true>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
+                     : launch_pdl(k_split_vel_tma<T, true, false>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m))
+         : (x.l2hint ? launch_pdl(k_split_vel_tma<T, false, true>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
+                     : launch_pdl(k_split_vel_tma<T, false, false>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m));
   return cuda_check(e, "split velocity (TMA) launch");
 }
 
@@ -732,6 +739,7 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   x.tnt = (s && s->nrec) ? s->traces_nt : 0;
   x.nrec = s ? s->nrec : 0;
   x.err = (int *)p->errflag;
+  x.l2hint = l2_hints_fit(5LL * c.nx * c.nz * (long long)sizeof(T), p->l2_bytes);
   // ISO/VTI: in place on the current psi set; TTI: from the current set
   // to the other one, every step
   T *psix0 = a.psix ? (T *)p->psix : nullptr, *psiz0 = a.psiz ? (T *)p->psiz : nullptr;

@@ -133,7 +133,7 @@ __device__ __forceinline__ Q4<T> mean4_fwd(const Q4<T> &a, T a4, const Q4<T> &b,
   return mul4(splat4<T>(T(0.25)), add4(add4(add4(a, next4(a, a4)), b), next4(b, b4)));
 }
 
-template <typename T, int NSLS>
+template <typename T, int NSLS, bool HINT>
 __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                       const SplitMaps &maps, int tile) {
   using G = SplitTtiGeom<T>;
@@ -232,8 +232,8 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   const bool surf = x.fs && gj == L;
   Q4<T> sxx = ldc4(a.sxx + g), szz = ldc4(a.szz + g), sxz = ldc4(a.sxz + g);
   // read once per step: streamed through L2 (ring-shared operands are not)
-  const Q4<T> C11 = ldgh4(a.c11 + g, l2_stream()), C13 = ldgh4(a.c13 + g, l2_stream()),
-              C33 = ldgh4(a.c33 + g, l2_stream());
+  const Q4<T> C11 = ldgh4(a.c11 + g, l2_stream_c<HINT>()), C13 = ldgh4(a.c13 + g, l2_stream_c<HINT>()),
+              C33 = ldgh4(a.c33 + g, l2_stream_c<HINT>());
   const Q4<T> c15a = ldg4(a.c15 + g), c15b = ldg4(a.c15 + g + nx);
   const Q4<T> c35a = ldg4(a.c35 + g), c35b = ldg4(a.c35 + g + nx);
   const Q4<T> c55a = ldg4(a.c55 + g), c55b = ldg4(a.c55 + g + nx);
@@ -262,10 +262,10 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
       const Q4<T> mx = ldc4(a.m + (0 * NSLS + n) * a.mstride + g);
       const Q4<T> mz = ldc4(a.m + (1 * NSLS + n) * a.mstride + g);
       const Q4<T> mq = ldc4(a.m + (2 * NSLS + n) * a.mstride + g);
-      sth4(a.m_o + (0 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxx, mul4(a2, mx)), mx), l2_stream());
+      sth4(a.m_o + (0 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxx, mul4(a2, mx)), mx), l2_stream_c<HINT>());
       sth4(a.m_o + (1 * NSLS + n) * a.mstride_o + g,
-           surf ? splat4<T>(0) : fma4(dt4, fma4(a1, rzz, mul4(a2, mz)), mz), l2_stream());
-      sth4(a.m_o + (2 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxz, mul4(a2, mq)), mq), l2_stream());
+           surf ? splat4<T>(0) : fma4(dt4, fma4(a1, rzz, mul4(a2, mz)), mz), l2_stream_c<HINT>());
+      sth4(a.m_o + (2 * NSLS + n) * a.mstride_o + g, fma4(dt4, fma4(a1, rxz, mul4(a2, mq)), mq), l2_stream_c<HINT>());
     }
   }
   for (int q = e0; q < e1; ++q) {  // explosive sources (after the force ones, before receivers)
@@ -279,9 +279,9 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   }
   if (surf) szz = splat4<T>(0);
   // sigma is re-read by the next velocity pass: keep it in L2
-  sth4(a.sxx + g, sxx, l2_keep());
-  sth4(a.szz + g, szz, l2_keep());
-  sth4(a.sxz + g, sxz, l2_keep());
+  sth4(a.sxx + g, sxx, l2_keep_c<HINT>());
+  sth4(a.szz + g, szz, l2_keep_c<HINT>());
+  sth4(a.sxz + g, sxz, l2_keep_c<HINT>());
   if (x.fs) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;
@@ -290,11 +290,11 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   }
 }
 
-template <typename T, int NSLS>
+template <typename T, int NSLS, bool HINT>
 __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
     k_split_stress_tti(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                        const __grid_constant__ SplitMaps maps) {
-  split_stress_tti_tile<T, NSLS>(a, x, maps, blockIdx.x);
+  split_stress_tti_tile<T, NSLS, HINT>(a, x, maps, blockIdx.x);
 }
 
 // Batched: one tile of one shot per CTA; the step parity selects the
@@ -306,25 +306,32 @@ __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 2
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  split_stress_tti_tile<T, NSLS>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  split_stress_tti_tile<T, NSLS, false>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
-template <typename T, int NSLS>
-static int launch_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
-                      cudaStream_t st, bool pdl) {
+template <typename T, int NSLS, bool HINT>
+static int launch_tti_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
+                        cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti<T, NSLS>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti<T, NSLS, HINT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split TTI stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress_tti<T, NSLS>, dim3(ntiles), dim3(G::NT),
+  return cuda_check(launch_pdl(k_split_stress_tti<T, NSLS, HINT>, dim3(ntiles), dim3(G::NT),
                                (size_t)G::SMEM, st, pdl, a, x, m),
                     "split TTI stress launch");
+}
+
+template <typename T, int NSLS>
+static int launch_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
+                      cudaStream_t st, bool pdl) {
+  return x.l2hint ? launch_tti_k<T, NSLS, true>(a, x, m, ntiles, st, pdl)
+                  : launch_tti_k<T, NSLS, false>(a, x, m, ntiles, st, pdl);
 }
 
 template <typename T>

@@ -106,6 +106,23 @@ __device__ __forceinline__ Q4<double> ldgh4(const double *p, uint64_t pol) {
   asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[2]), "=d"(q.v[3]) : "l"(p + 2), "l"(pol));
   return q;
 }
+// Policies fixed per kernel instantiation (the hints pay when the kept
+// set — the new v and sigma — fits in half the L2; beyond that kept lines
+// thrash each other): with ON false both are evict_normal, so the accesses
+// behave as plain ones.
+__device__ __forceinline__ uint64_t l2_normal() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+template <bool ON>
+__device__ __forceinline__ uint64_t l2_keep_c() {
+  return ON ? l2_keep() : l2_normal();
+}
+template <bool ON>
+__device__ __forceinline__ uint64_t l2_stream_c() {
+  return ON ? l2_stream() : l2_normal();
+}
 __device__ __forceinline__ void stg4(float *p, const Q4<float> &q) {
   *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
 }
