@@ -20,11 +20,19 @@
 // (2048 x 1024 VTI: 29.4 vs 28.0 Gpt/s on B200).  Issuing the independent
 // loads (sigma, M, medium) before the wait measured slower.
 //
-// Each cell's operands cross HBM once per kernel: 8 planes for the velocity
-// kernel (sigma 3 + v 2 + rho read, v written) and 2 + 2*(3 + 3N) + N_m for
-// the stress kernel — 156 B per point per step for FP32 VTI with 3 SLS
-// against 136 B for a single fused pass, but with a fraction of the fused
-// kernel's arithmetic per byte.
+// Each cell's operands cross the SMs' ports once per kernel: 8 planes for
+// the velocity kernel (sigma 3 + v 2 + rho read, v written) and
+// 2 + 2*(3 + 3N) + N_m for the stress kernel — 156 B per point per step
+// for FP32 VTI with 3 SLS against 136 B for a single fused pass, but with
+// a fraction of the fused kernel's arithmetic per byte.  When the new v
+// and sigma fit in half the L2, their stores are marked evict_last and the
+// memory variables and once-read stiffnesses evict_first (the HINT
+// template parameter), so the other pass of the step finds v and sigma in
+// L2: 235 MB per step then reach DRAM on 2048 x 1024 against 290 MB of
+// operands (37.5 vs 35.0 Gpt/s).
+// Every launch with an explicit program order: the out-of-place forms
+// (OOP: state read from one buffer, written to another) serve the
+// gradient's segment recompute.
 // In place is safe for ISO/VTI: the velocity kernel reads v only at its own
 // cells and never writes sigma; the stress kernel reads v and writes sigma,
 // M and psi only at its own cells.  The TTI stress pass also reads M and
@@ -192,7 +200,8 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
 }
 
 // Tile height of the TMA-staged velocity pass (64 x 8: 34.8 Gpt/s on the
-// 2048 x 1024 VTI step; 64 x 16: 34.3; 64 x 32: 33.0).
+// 2048 x 1024 VTI step; 64 x 16: 34.3; 64 x 32: 33.0; with the L2 hints
+// 64 x 8: 37.6, 64 x 16: 37.0).
 constexpr int kVelTmaTZ = 8;
 
 // Velocity pass with the stress taps staged by TMA (the default): one
