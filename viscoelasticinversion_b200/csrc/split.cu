@@ -30,9 +30,8 @@
 // template parameter), so the other pass of the step finds v and sigma in
 // L2: 235 MB per step then reach DRAM on 2048 x 1024 against 290 MB of
 // operands (37.5 vs 35.0 Gpt/s).
-// Every launch with an explicit program order: the out-of-place forms
-// (OOP: state read from one buffer, written to another) serve the
-// gradient's segment recompute.
+// The out-of-place forms (OOP: the state read from one buffer and written
+// to another) serve the gradient's segment recompute.
 // In place is safe for ISO/VTI: the velocity kernel reads v only at its own
 // cells and never writes sigma; the stress kernel reads v and writes sigma,
 // M and psi only at its own cells.  The TTI stress pass also reads M and
