@@ -91,21 +91,29 @@ __device__ __forceinline__ void tti_rates4(const StepArgs<T> &a, const T *s_vx, 
   rxz = add4(dzvx, dxvz);
 }
 
-// Effective SLS rates e = (1 + tau) r + tau * sum_n M_n of 4 cells whose
-// memory variables start at m (plane stride ms).
+// Sums over the SLS of the memory variables (xx, zz, xz) of 4 cells whose
+// memory variables start at m (plane stride ms).  They do not depend on the
+// new velocities, so they are loaded while the velocity box is in flight.
 template <typename T, int NSLS>
-__device__ __forceinline__ void tti_effective4(const T *m, long long ms, long long g,
-                                               const Q4<T> &tau, const Q4<T> &rxx,
-                                               const Q4<T> &rzz, const Q4<T> &rxz, Q4<T> &exx,
-                                               Q4<T> &ezz, Q4<T> &exz) {
-  if constexpr (NSLS > 0) {
-    Q4<T> Sxx = ldc4(m + g), Szz = ldc4(m + NSLS * ms + g), Sxz = ldc4(m + 2 * NSLS * ms + g);
+__device__ __forceinline__ void tti_msum4(const T *m, long long ms, long long g, Q4<T> &Sxx,
+                                          Q4<T> &Szz, Q4<T> &Sxz) {
+  Sxx = Szz = Sxz = splat4<T>(0);
 #pragma unroll
-    for (int n = 1; n < NSLS; ++n) {
-      Sxx = add4(Sxx, ldc4(m + n * ms + g));
-      Szz = add4(Szz, ldc4(m + (NSLS + n) * ms + g));
-      Sxz = add4(Sxz, ldc4(m + (2 * NSLS + n) * ms + g));
-    }
+  for (int n = 0; n < NSLS; ++n) {
+    Sxx = add4(Sxx, ldc4(m + n * ms + g));
+    Szz = add4(Szz, ldc4(m + (NSLS + n) * ms + g));
+    Sxz = add4(Sxz, ldc4(m + (2 * NSLS + n) * ms + g));
+  }
+}
+
+// Effective SLS rates e = (1 + tau) r + tau * sum_n M_n of 4 cells.
+template <typename T, int NSLS>
+__device__ __forceinline__ void tti_effective4(const Q4<T> &tau, const Q4<T> &Sxx,
+                                               const Q4<T> &Szz, const Q4<T> &Sxz,
+                                               const Q4<T> &rxx, const Q4<T> &rzz,
+                                               const Q4<T> &rxz, Q4<T> &exx, Q4<T> &ezz,
+                                               Q4<T> &exz) {
+  if constexpr (NSLS > 0) {
     const Q4<T> t1 = add4(tau, splat4<T>(T(1)));
     exx = fma4(t1, rxx, mul4(tau, Sxx));
     ezz = fma4(t1, rzz, mul4(tau, Szz));
@@ -177,6 +185,10 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   const long long rg = (long long)rgj * nx + rgi0;
   Q4<T> rtau = splat4<T>(0);
   if (ract && NSLS > 0) rtau = ldg4(a.tau + rg);
+  // while the box is in flight: the memory-variable sums into registers
+  Q4<T> mxx = splat4<T>(0), mzz = mxx, mxz = mxx, qmxx = mxx, qmzz = mxx, qmxz = mxx;
+  if (act) tti_msum4<T, NSLS>(a.m, a.mstride, g, mxx, mzz, mxz);
+  if (ract) tti_msum4<T, NSLS>(a.m, a.mstride, rg, qmxx, qmzz, qmxz);
   const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
   const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
   if (__syncthreads_or(!ok)) {
@@ -192,7 +204,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
     Q4<T> exx = splat4<T>(0), ezz = exx, exz = exx;
     if (act) {
       tti_rates4<T, BW>(a, s_vx, s_vz, (r + 5) * BW + lx + 4, gi0, gj, true, rxx, rzz, rxz);
-      tti_effective4<T, NSLS>(a.m, a.mstride, g, tau, rxx, rzz, rxz, exx, ezz, exz);
+      tti_effective4<T, NSLS>(tau, mxx, mzz, mxz, rxx, rzz, rxz, exx, ezz, exz);
     }
     const int e = (r + 1) * EW + lx + 4;
     stg4(s_exx + e, exx);
@@ -204,7 +216,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
     if (ract) {
       Q4<T> qxx, qzz, qxz;
       tti_rates4<T, BW>(a, s_vx, s_vz, (rr + 4) * BW + rc, rgi0, rgj, false, qxx, qzz, qxz);
-      tti_effective4<T, NSLS>(a.m, a.mstride, rg, rtau, qxx, qzz, qxz, exx, ezz, exz);
+      tti_effective4<T, NSLS>(rtau, qmxx, qmzz, qmxz, qxx, qzz, qxz, exx, ezz, exz);
     }
     const int e = rr * EW + rc;
     stg4(s_exx + e, exx);
