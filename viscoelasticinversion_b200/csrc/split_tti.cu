@@ -10,7 +10,8 @@
 // variables and CPML psi at the same time, so M and psi are read from one
 // buffer and written to the other (ping-pong per step); sigma is read and
 // written only at the CTA's own cells, in place.  The velocity pass is the
-// medium-independent k_split_vel_ldg.
+// medium-independent one of split.cu (k_split_vel_tma by default), with psi
+// read from one set and written to the other.
 #include <atomic>
 #include <cudaTypedefs.h>
 
