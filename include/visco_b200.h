@@ -271,12 +271,13 @@ int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const 
 
 /* ---- request server ---------------------------------------------------- */
 /* Forward solves and misfit gradients submitted from any host thread and
- * run by one worker thread on its own stream.  The reference solves one
- * problem per call and has no server (ViscoelasticProblem.jl:273-309).
- * Admission against an HBM budget; requests join and leave between slices
- * of slice_steps steps (continuous batching), each slice going to the
- * resident request with the least remaining work (cells x steps left), so
- * short requests preempt long ones; gradient requests run whole.
+ * run by `lanes` worker threads, each resident request on its own stream.
+ * The reference solves one problem per call and has no server
+ * (ViscoelasticProblem.jl:273-309).  Admission against an HBM budget;
+ * requests join and leave between slices of slice_steps steps (continuous
+ * batching), each idle lane taking the next slice of the idle resident
+ * request with the least remaining work (cells x steps left), so short
+ * requests preempt long ones; gradient requests run whole.
  * Every request has its own plan: its results equal a vi_forward_host /
  * vi_gradient call on the same inputs, whatever else is resident. */
 typedef struct vi_server vi_server;
