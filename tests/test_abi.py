@@ -70,3 +70,13 @@ def test_cfl_violation_is_reported_before_any_device_work():
     assert _abi.lib().vi_plan_create(C.byref(cfg), C.byref(h)) == _abi.VI_ERR_CFL
     with pytest.raises(_abi.CFLError):
         _abi.check(_abi.VI_ERR_CFL)
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No fallback: without the built library every call path raises."""
+    monkeypatch.setattr(_abi, "LIB_PATH", tmp_path / "libvisco_b200.so")
+    monkeypatch.setattr(_abi, "_lib", None)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        _abi.lib()
+    with pytest.raises(RuntimeError, match="not built"):
+        _abi.check(_abi.VI_ERR_ARG)
