@@ -268,6 +268,14 @@ int vi_gradient(vi_plan *plan, const vi_medium *med_dev, const vi_shot *shot, in
 int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const double *vp,
                          const double *vs, const double *rho, const double *eps,
                          const double *delta, double tau_scale, double *out4, void *stream);
+/* VTI: from the same grad planes to the Thomsen parameters at fixed vp,
+ * vs, rho: out2 = [dJ/d(epsilon), dJ/d(delta)] (C11 = C33 (1 + 2 epsilon),
+ * C13 from delta as in Models.jl:27-52; custom_solver/Model.jl:12-16
+ * carries epsilon, delta, gamma).  gamma enters only SH motion, so dJ/dgamma
+ * is zero in 2D P-SV and not written.  delta NULL means 0.  FP64 device
+ * planes of np cells; asynchronous on `stream`. */
+int vi_gradient_thomsen(int64_t np, const double *grad8, const double *vp, const double *vs,
+                        const double *rho, const double *delta, double *out2, void *stream);
 
 /* ---- request server ---------------------------------------------------- */
 /* Forward solves and misfit gradients submitted from any host thread and

@@ -3,7 +3,8 @@ central finite differences of the FP64 oracle's misfit — directional
 derivatives of every medium plane (along the gradient and along a bump
 between source and receivers), and single-cell derivatives at 20 seeded
 cells — plus checkpoint-interval
-independence, FP32 vs FP64, and the (vp, vs, rho, 1/Q) chain rule.
+independence, FP32 vs FP64, and the (vp, vs, rho, 1/Q) and Thomsen
+(epsilon, delta) chain rules.
 
 The reference has no gradient to compare with (no Enzyme call exists); the
 oracle's finite differences stand in for it."""
@@ -14,7 +15,8 @@ import pytest
 import torch
 
 from viscoelasticinversion_b200 import StepPlan, media
-from viscoelasticinversion_b200.gradient import GRADIENT_PLANES, misfit_gradient, velocity_gradient
+from viscoelasticinversion_b200.gradient import (GRADIENT_PLANES, misfit_gradient, thomsen_gradient,
+                                                 velocity_gradient)
 from tests.helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -197,4 +199,41 @@ def test_velocity_chain_rule(oracle_lib, kind):
 
         fd = _richardson(J_of)
         an = float(np.sum(gv[n] * d))
+        assert abs(fd - an) <= FD_REL_TOL * abs(an), (name, fd, an)
+
+
+def test_thomsen_chain_rule(oracle_lib):
+    """dJ/d(epsilon, delta) of a VTI medium at fixed vp, vs, rho and Q
+    (vi_gradient_thomsen): against the chain rule restated in numpy, and
+    against central differences of the oracle's misfit along the gradient."""
+    w = _vti()
+    qf = media.q_fit(*w.meta["band"], w.nsls)
+    fields = dict(w.meta["fields"])
+
+    def build(f):
+        return _with(w, **media.medium_from_velocity("vti", f["vp"], f["vs"], f["rho"], f["eps"],
+                                                     f["delta"], f["Q"], qf))
+
+    w = build(fields)
+    obs, _ = oracle_lib.run(_truth(w), precision="f64")
+    _, g = _gpu_gradient(w, obs)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    vp, vs, rho, dlt = fields["vp"], fields["vs"], fields["rho"], fields["delta"]
+    gt = thomsen_gradient(dev(g), dev(vp), dev(vs), dev(rho), dev(dlt)).cpu().numpy()
+    C33, C55 = rho * vp**2, rho * vs**2
+    A, B = C33 - C55, C33 * (1 + 2 * dlt) - C55
+    ref = np.stack([g[GRADIENT_PLANES.index("c11")] * 2 * C33,
+                    g[GRADIENT_PLANES.index("c13")] * A * C33 / np.sqrt(A * B)])
+    assert rel_l2(gt, ref) <= 1e-13
+    for n, name in enumerate(("eps", "delta")):
+        base = fields[name]
+        d = 1e-4 * np.abs(base).max() * gt[n] / np.abs(gt[n]).max()
+
+        def J_of(h):
+            f = dict(fields)
+            f[name] = base + h * d
+            return _oracle_J(oracle_lib, build(f), obs)
+
+        fd = _richardson(J_of)
+        an = float(np.sum(gt[n] * d))
         assert abs(fd - an) <= FD_REL_TOL * abs(an), (name, fd, an)

@@ -155,6 +155,8 @@ _SIGNATURES = [
     ("vi_gradient_velocity", C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                        C.c_void_p, C.c_void_p]),
+    ("vi_gradient_thomsen", C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
 
 VI_BATCH_NO_GRAPH = 1

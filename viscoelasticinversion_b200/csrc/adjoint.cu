@@ -23,7 +23,8 @@
 //
 // Gradients are with respect to the medium planes (rho, c11, c13, c33,
 // c55, tau) — for ISO c13 = lambda and c55 = mu carry dJ/dlambda and
-// dJ/dmu.  vi_gradient_velocity maps them to (vp, vs, rho, 1/Q).
+// dJ/dmu.  vi_gradient_velocity maps them to (vp, vs, rho, 1/Q) and, for
+// VTI, vi_gradient_thomsen to the Thomsen (epsilon, delta).
 #include <cmath>
 #include <vector>
 
@@ -573,6 +574,24 @@ __global__ void k_velocity_grad(int kind, long long np, const double *g, const d
   out[3 * np + c] = gtau * tau_scale;                 // dJ/d(1/Q)
 }
 
+// VTI Thomsen parameters at fixed (vp, vs, rho): C11 = C33 (1 + 2 eps)
+// gives dC11/deps = 2 C33; C13 = sqrt(A B) - C55 with A = C33 - C55,
+// B = C33 (1 + 2 delta) - C55 gives dC13/ddelta = A C33 / sqrt(A B)
+// (media.thomsen_vti; custom_solver/Model.jl:12-16).  gamma enters only SH
+// motion: no 2D P-SV stiffness depends on it.
+__global__ void k_thomsen_grad(long long np, const double *g, const double *vp, const double *vs,
+                               const double *rho, const double *delta, double *out) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= np) return;
+  const double g11 = g[1 * np + c], g13 = g[2 * np + c];
+  const double r = rho[c], C33 = r * vp[c] * vp[c], C55 = r * vs[c] * vs[c];
+  const double d = delta ? delta[c] : 0.0;
+  const double A = C33 - C55, B = C33 * (1 + 2 * d) - C55;
+  const double sq = sqrt(fmax(A * B, 1e-300));
+  out[0 * np + c] = g11 * 2 * C33;     // dJ/deps
+  out[1 * np + c] = g13 * A * C33 / sq;  // dJ/ddelta
+}
+
 __global__ void k_fold_iso(long long np, double *g) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= np) return;
@@ -862,4 +881,13 @@ extern "C" int vi_gradient_velocity(int32_t medium, int64_t np, const double *gr
   k_velocity_grad<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       medium, np, grad8, vp, vs, rho, eps, delta, tau_scale, out4);
   return cuda_check(cudaGetLastError(), "gradient_velocity launch");
+}
+
+extern "C" int vi_gradient_thomsen(int64_t np, const double *grad8, const double *vp, const double *vs,
+                                   const double *rho, const double *delta, double *out2, void *stream) {
+  if (!grad8 || !vp || !vs || !rho || !out2 || np <= 0)
+    return set_error(VI_ERR_ARG, "gradient_thomsen: NULL argument");
+  k_thomsen_grad<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(np, grad8, vp, vs, rho,
+                                                                                 delta, out2);
+  return cuda_check(cudaGetLastError(), "gradient_thomsen launch");
 }

@@ -79,6 +79,29 @@ def velocity_gradient(kind: str, grad: torch.Tensor, vp: torch.Tensor, vs: torch
     return out
 
 
+def thomsen_gradient(grad: torch.Tensor, vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tensor,
+                     delta: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """[2, nz, nx] float64: dJ/d(epsilon, delta) of a VTI medium at fixed
+    vp, vs, rho, from the stiffness gradient (C11 = C33 (1 + 2 epsilon),
+    C13 from delta: media.thomsen_vti).  gamma, the third Thomsen parameter
+    of custom_solver/Model.jl:12-16, enters only SH motion: its gradient is
+    zero in 2D P-SV."""
+    np_ = grad.shape[1] * grad.shape[2]
+    out = torch.empty(2, grad.shape[1], grad.shape[2], dtype=torch.float64, device=grad.device)
+
+    def p(t):
+        if t is None:
+            return None
+        if t.dtype != torch.float64 or not t.is_contiguous() or t.numel() != np_:
+            raise ValueError("velocity planes must be contiguous float64 [nz, nx]")
+        return t.data_ptr()
+
+    with torch.cuda.device(grad.device):
+        check(lib().vi_gradient_thomsen(np_, grad.data_ptr(), p(vp), p(vs), p(rho), p(delta),
+                                        out.data_ptr(), _stream_handle(stream)))
+    return out
+
+
 def shard(nshots: int, rank: int, world: int) -> list[int]:
     """Shots of this rank: round robin, so uneven shot costs spread."""
     return list(range(rank, nshots, world))
