@@ -15,8 +15,8 @@ import pytest
 import torch
 
 from viscoelasticinversion_b200 import StepPlan, media
-from viscoelasticinversion_b200.gradient import (GRADIENT_PLANES, misfit_gradient, thomsen_gradient,
-                                                 velocity_gradient)
+from viscoelasticinversion_b200.gradient import (GRADIENT_PLANES, misfit_gradient, shot_misfit,
+                                                 thomsen_gradient, velocity_gradient)
 from tests.helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -237,3 +237,34 @@ def test_thomsen_chain_rule(oracle_lib):
         fd = _richardson(J_of)
         an = float(np.sum(gt[n] * d))
         assert abs(fd - an) <= FD_REL_TOL * abs(an), (name, fd, an)
+
+
+def test_autograd_function(oracle_lib):
+    """shot_misfit as a torch autograd function: J and the plane gradients
+    equal misfit_gradient's, and J backpropagates through torch ops from vp
+    (ISO: lambda = rho (vp^2 - 2 vs^2), mu = rho vs^2) to the dJ/dvp of
+    vi_gradient_velocity."""
+    w = _iso(nt=160)
+    obs_np, _ = oracle_lib.run(_truth(w), precision="f64")
+    plan = StepPlan.for_workload(w, "f64")
+    wav = torch.as_tensor(w.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
+    obs = torch.as_tensor(obs_np, dtype=plan.dtype, device=plan.device).contiguous()
+    med = {k: v.clone().requires_grad_(True) for k, v in plan.medium_to_device(w.medium).items()}
+    J = shot_misfit(plan, med, w.sources, wav, w.receivers, obs)
+    J.backward()
+    J0, g0 = misfit_gradient(plan, {k: v.detach() for k, v in med.items()}, w.sources, wav,
+                             w.receivers, obs)
+    assert J0 > 0 and abs(float(J.detach()) - J0) <= 1e-13 * J0
+    for k, v in med.items():
+        ref = g0[GRADIENT_PLANES.index(k)]
+        assert rel_l2(v.grad.cpu().numpy(), ref.cpu().numpy()) <= 1e-13, k
+    shape = (w.nz, w.nx)
+    rho, tau = med["rho"].detach(), med["tau"].detach()
+    vs = torch.full(shape, 1732.0, dtype=torch.float64, device=plan.device)
+    vp = torch.full(shape, 3000.0, dtype=torch.float64, device=plan.device, requires_grad=True)
+    J2 = shot_misfit(plan, {"rho": rho, "c13": rho * (vp**2 - 2 * vs**2), "c55": rho * vs**2,
+                            "tau": tau}, w.sources, wav, w.receivers, obs)
+    J2.backward()
+    gv = velocity_gradient("iso", g0, vp.detach(), vs, rho)
+    assert rel_l2(vp.grad.cpu().numpy(), gv[0].cpu().numpy()) <= 1e-12
+    plan.close()

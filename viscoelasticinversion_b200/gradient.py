@@ -6,7 +6,8 @@ takes a `grad_fn` and a `loss_fn` and is never wired to the wave solver
 (examples/energy_natural_gradient_example.jl:252-315).  `misfit_gradient`
 is that grad_fn for the leapfrog step: J = 1/2 sum (d - obs)^2 over the vx
 and vz traces and dJ/d(medium planes), by the discrete adjoint of the step
-in libvisco_b200.so.  `shot_gradient` sums over shots, sharded by shot over
+in libvisco_b200.so; `shot_misfit` wraps it as a torch autograd function.
+`shot_gradient` sums over shots, sharded by shot over
 the ranks of a process group with one FP64 all-reduce of the gradient
 planes and the misfit.
 """
@@ -53,6 +54,42 @@ def misfit_gradient(plan: StepPlan, medium: dict, sources, wavelets, receivers, 
                                 C.byref(J), _stream_handle(stream)))
     del keep
     return J.value, grad
+
+
+class ShotMisfit(torch.autograd.Function):
+    """The misfit J(medium) of one shot as a torch autograd function, the
+    counterpart of a ChainRulesCore.rrule on the Julia side: forward runs
+    vi_gradient, which yields J and dJ/d(medium planes) in one forward and
+    adjoint pass, and keeps the gradient; backward scales it by the incoming
+    cotangent.  Use through `shot_misfit`."""
+
+    @staticmethod
+    def forward(ctx, plan, sources, wavelets, receivers, obs, checkpoint_every, names, *planes):
+        J, g = misfit_gradient(plan, dict(zip(names, planes)), sources, wavelets, receivers, obs,
+                               checkpoint_every=checkpoint_every)
+        ctx.names = names
+        ctx.dtypes = [t.dtype for t in planes]
+        ctx.save_for_backward(g)
+        return torch.tensor(J, dtype=torch.float64, device=g.device)
+
+    @staticmethod
+    def backward(ctx, gJ):
+        (g,) = ctx.saved_tensors
+        grads = [(gJ * g[GRADIENT_PLANES.index(n)]).to(dt) for n, dt in zip(ctx.names, ctx.dtypes)]
+        return (None,) * 7 + tuple(grads)
+
+
+def shot_misfit(plan: StepPlan, medium: dict, sources, wavelets, receivers, obs: torch.Tensor,
+                checkpoint_every: int = 0) -> torch.Tensor:
+    """J of one shot (0-d float64 tensor) differentiable with respect to
+    every medium plane given (device tensors in the plan's precision, keys
+    of GRADIENT_PLANES), so that J.backward() reaches parameters the planes
+    were computed from in torch (velocities, Thomsen parameters, 1/Q)."""
+    names = tuple(k for k in GRADIENT_PLANES if k in medium)
+    if set(names) != set(medium):
+        raise ValueError(f"medium keys must be among {GRADIENT_PLANES}")
+    return ShotMisfit.apply(plan, sources, wavelets, receivers, obs, int(checkpoint_every), names,
+                            *[medium[n].contiguous() for n in names])
 
 
 def velocity_gradient(kind: str, grad: torch.Tensor, vp: torch.Tensor, vs: torch.Tensor,
