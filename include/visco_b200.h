@@ -277,6 +277,23 @@ int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const 
 int vi_gradient_thomsen(int64_t np, const double *grad8, const double *vp, const double *vs,
                         const double *rho, const double *delta, double *out2, void *stream);
 
+/* ---- medium parameterisation ------------------------------------------ */
+/* Writes the medium planes the step reads from FP64 parameter planes of np
+ * cells on the device: ISO rho, c13 = lambda = rho (vp^2 - 2 vs^2), c55 =
+ * mu = rho vs^2; VTI rho, c11, c13, c33, c55 from Thomsen epsilon, delta
+ * (Models.jl:27-52, custom_solver/Model.jl:12-16); TTI the VTI stiffness
+ * tilted by theta (radians, symmetry axis from z towards x; 2D Bond
+ * rotation) into c11, c13, c15, c33, c35, c55.  With q (the quality factor
+ * plane) also tau = tau_scale / q, tau_scale = N / Kbar of the Q fit
+ * (Models.jl:67).  eps, delta, theta NULL mean 0.  `out` names the device
+ * planes to write, in `precision` (VI_F32 / VI_F64); those the medium kind
+ * needs must be non-NULL.  Asynchronous on `stream`.  The reference does
+ * this on the host before every solve. */
+int vi_medium_from_velocity(int32_t medium, int32_t precision, int64_t np, const double *vp,
+                            const double *vs, const double *rho, const double *eps,
+                            const double *delta, const double *theta, const double *q,
+                            double tau_scale, const vi_medium *out, void *stream);
+
 /* ---- request server ---------------------------------------------------- */
 /* Forward solves and misfit gradients submitted from any host thread and
  * run by `lanes` worker threads, each resident request on its own stream.

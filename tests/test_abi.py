@@ -80,3 +80,21 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
         _abi.lib()
     with pytest.raises(RuntimeError, match="not built"):
         _abi.check(_abi.VI_ERR_ARG)
+
+
+def test_medium_from_velocity_argument_checks():
+    """Argument errors are found before any device work (no GPU needed)."""
+    lib = _abi.lib()
+    dummy = C.c_void_p(16)  # never dereferenced: the checks fail first
+    out = _abi.ViMedium()
+    out.rho = out.c55 = 16  # c13 missing
+    rc = lib.vi_medium_from_velocity(_abi.VI_MEDIUM_ISO, _abi.VI_F32, 10, dummy, dummy, dummy, None,
+                                     None, None, None, 0.0, C.byref(out), None)
+    assert rc == _abi.VI_ERR_ARG and b"NULL" in lib.vi_last_error()
+    out.c13 = 16
+    rc = lib.vi_medium_from_velocity(_abi.VI_MEDIUM_ISO, 7, 10, dummy, dummy, dummy, None, None,
+                                     None, None, 0.0, C.byref(out), None)
+    assert rc == _abi.VI_ERR_ARG and b"precision" in lib.vi_last_error()
+    rc = lib.vi_medium_from_velocity(_abi.VI_MEDIUM_VTI, _abi.VI_F32, 10, dummy, dummy, dummy, None,
+                                     None, None, None, 0.0, C.byref(out), None)
+    assert rc == _abi.VI_ERR_ARG  # VTI needs c11 and c33

@@ -157,6 +157,9 @@ _SIGNATURES = [
                                        C.c_void_p, C.c_void_p]),
     ("vi_gradient_thomsen", C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("vi_medium_from_velocity", C.c_int, [C.c_int32, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_double, C.POINTER(ViMedium), C.c_void_p]),
 ]
 
 VI_BATCH_NO_GRAPH = 1
