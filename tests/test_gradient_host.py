@@ -1,7 +1,9 @@
-"""Host logic of gradient.shot_misfit (CPU, no GPU): the autograd function
-maps each medium plane to its gradient plane and scales by the cotangent.
-vi_gradient is replaced by a stand-in with a known gradient; the real one is
-checked against the oracle in test_gpu_gradient.py."""
+"""Host logic on the CPU (no GPU): gradient.shot_misfit, the autograd
+function, maps each medium plane to its gradient plane and scales by the
+cotangent (vi_gradient replaced by a stand-in with a known gradient; the
+real one is checked against the oracle in test_gpu_gradient.py); the
+device parameterisation wrapper checks its arguments before any device
+work."""
 import pytest
 import torch
 
@@ -38,3 +40,13 @@ def test_shot_misfit_backward_through_torch(monkeypatch):
 def test_shot_misfit_rejects_unknown_planes():
     with pytest.raises(ValueError, match="medium keys"):
         G.shot_misfit(None, {"lambda": torch.zeros(2, 2)}, [], None, [], None)
+
+
+def test_device_parameterisation_checks_arguments_before_device_work():
+    from viscoelasticinversion_b200.param import medium_from_velocity_device
+
+    z = torch.zeros(3, 4, dtype=torch.float64)
+    with pytest.raises(ValueError, match="kind"):
+        medium_from_velocity_device("ortho", z, z, z)
+    with pytest.raises(ValueError, match="tau_scale"):
+        medium_from_velocity_device("iso", z, z, z, Q=z)
