@@ -29,7 +29,7 @@ import torch
 
 from . import media as _media
 from .batch import ShotBatch
-from .gradient import GRADIENT_PLANES, misfit_gradient
+from .gradient import GRADIENT_PLANES, misfit_gradient, shard
 from .solver import StepPlan
 
 
@@ -171,10 +171,15 @@ class FWIProblem:
     planes stay as in `base`.  `shots` are workloads on base's grid (their
     own sources, wavelets, receivers, nt) and `obs` their observed traces
     ([2, nrec, nt] each).  loss(θ) = Σ_shots J, grad(θ) = dloss/dθ by
-    vi_gradient; batch_loss evaluates many θ for all shots as one vi_batch."""
+    vi_gradient; batch_loss evaluates many θ for all shots as one vi_batch.
+
+    Under torch.distributed each rank evaluates its round-robin share of the
+    shots and one FP64 all-reduce sums the misfit with the gradient (or the
+    line search's losses), so every rank holds the same sums and takes the
+    same optimizer step; only the ranks' share of `obs` is read."""
 
     def __init__(self, base: _media.Workload, shots, obs, planes=("c13", "c55"),
-                 precision: str = "f64", checkpoint_every: int = 0):
+                 precision: str = "f64", checkpoint_every: int = 0, group=None):
         unknown = [k for k in planes if k not in GRADIENT_PLANES or k not in base.medium]
         if unknown:
             raise ValueError(f"planes not in the medium: {unknown}")
@@ -188,7 +193,18 @@ class FWIProblem:
         self.precision, self.checkpoint_every = precision, int(checkpoint_every)
         self.np = base.nx * base.nz
         self.n_params = len(self.planes) * self.np
-        self.plan = StepPlan.for_workload(base, precision)
+        self.group = group
+        rank, world = 0, 1
+        if torch.distributed.is_available() and torch.distributed.is_initialized():
+            rank, world = torch.distributed.get_rank(group), torch.distributed.get_world_size(group)
+        self.mine = shard(len(self.shots), rank, world)
+        self._plan = None
+
+    @property
+    def plan(self) -> StepPlan:
+        if self._plan is None:
+            self._plan = StepPlan.for_workload(self.base, self.precision)
+        return self._plan
 
     def medium(self, theta) -> dict:
         theta = np.asarray(theta, dtype=np.float64).reshape(len(self.planes), self.base.nz, self.base.nx)
@@ -197,46 +213,70 @@ class FWIProblem:
             med[k] = self.base.medium[k] * (1.0 + theta[n])
         return med
 
-    def _value_and_grad(self, theta):
+    # per-shot work on this rank's GPU
+    def _shots_value_and_grad(self, theta, shots):
+        """(Σ J, Σ dJ/dplane [8, nz, nx] float64 numpy) over the given shots."""
         plan, dev = self.plan, self.plan.device
         med = plan.medium_to_device(self.medium(theta))
-        g = None
+        g = torch.zeros(8, self.base.nz, self.base.nx, dtype=torch.float64, device=dev)
         J = 0.0
-        for w, o in zip(self.shots, self.obs):
+        for i in shots:
+            w = self.shots[i]
             wav = torch.as_tensor(w.wavelets[:, :w.nt], dtype=plan.dtype, device=dev).contiguous()
-            obs = torch.as_tensor(o, dtype=plan.dtype, device=dev).contiguous()
+            obs = torch.as_tensor(self.obs[i], dtype=plan.dtype, device=dev).contiguous()
             Jw, g = misfit_gradient(plan, med, w.sources, wav, w.receivers, obs, nt=w.nt,
-                                    checkpoint_every=self.checkpoint_every, grad=g,
-                                    accumulate=g is not None)
+                                    checkpoint_every=self.checkpoint_every, grad=g, accumulate=True)
             J += Jw
-        # plane = base · (1 + θ): dJ/dθ = dJ/dplane · base
-        gp = np.stack([g[GRADIENT_PLANES.index(k)].cpu().numpy() * self.base.medium[k]
-                       for k in self.planes])
-        return J, gp.ravel()
+        return J, g.cpu().numpy()
 
-    def loss(self, theta) -> float:
-        return self._value_and_grad(theta)[0]
-
-    def grad(self, theta) -> np.ndarray:
-        return self._value_and_grad(theta)[1]
-
-    def batch_loss(self, thetas) -> list:
-        """Σ_shots J for every θ, all (θ, shot) pairs as one batched run."""
-        ws = [dataclasses.replace(w, medium=self.medium(t)) for t in thetas for w in self.shots]
+    def _shots_batch_loss(self, thetas, shots) -> np.ndarray:
+        """Σ_shots J for every θ over the given shots, as one batched run."""
+        if not shots:
+            return np.zeros(len(thetas))
+        ws = [dataclasses.replace(self.shots[i], medium=self.medium(t)) for t in thetas for i in shots]
         b = ShotBatch(ws, self.precision)
         try:
             b.run()
             b.status()
-            out = []
-            for i in range(len(thetas)):
-                J = 0.0
-                for s, o in enumerate(self.obs):
-                    d = b.traces[i * len(self.shots) + s].double()
-                    J += 0.5 * float(torch.sum((d - torch.as_tensor(o, device=d.device)) ** 2))
-                out.append(J)
+            out = np.zeros(len(thetas))
+            for n in range(len(thetas)):
+                for k, i in enumerate(shots):
+                    d = b.traces[n * len(shots) + k].double()
+                    o = torch.as_tensor(self.obs[i], device=d.device)
+                    out[n] += 0.5 * float(torch.sum((d - o) ** 2))
             return out
         finally:
             b.close()
 
+    # sums over every shot (all ranks)
+    def _allreduce(self, flat: np.ndarray) -> np.ndarray:
+        if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+            return flat
+        t = torch.as_tensor(flat, dtype=torch.float64)
+        if torch.distributed.get_backend(self.group) == "nccl":
+            t = t.to(self.plan.device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM, group=self.group)
+        return t.cpu().numpy()
+
+    def value_and_grad(self, theta):
+        J, g = self._shots_value_and_grad(theta, self.mine)
+        # plane = base · (1 + θ): dJ/dθ = dJ/dplane · base
+        gp = np.stack([g[GRADIENT_PLANES.index(k)] * self.base.medium[k] for k in self.planes])
+        tot = self._allreduce(np.concatenate([gp.ravel(), [J]]))
+        return float(tot[-1]), tot[:-1]
+
+    def loss(self, theta) -> float:
+        return self.value_and_grad(theta)[0]
+
+    def grad(self, theta) -> np.ndarray:
+        return self.value_and_grad(theta)[1]
+
+    def batch_loss(self, thetas) -> list:
+        """Σ_shots J for every θ: this rank's shots as one batched run, then
+        one all-reduce of the losses."""
+        return list(self._allreduce(self._shots_batch_loss(thetas, self.mine)))
+
     def close(self):
-        self.plan.close()
+        if self._plan is not None:
+            self._plan.close()
+            self._plan = None
