@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -58,6 +59,7 @@ namespace vb {
 constexpr int kFormOneStage = 0, kFormTwoStage = 1, kFormSplit = 2, kFormPerShot = 3;
 
 static std::map<std::string, int> g_tuned;  // kernel form chosen per problem class
+static std::mutex g_tuned_mu;               // batches may run on several host threads
 
 static std::string tune_key(const vi_batch *b) {
   std::vector<std::pair<int, int>> g;
@@ -329,10 +331,13 @@ static int time_marginal(F run_steps, cudaStream_t st, int max_nt, float *ms) {
 template <typename T>
 static int tune(vi_batch *b, cudaStream_t st) {
   const std::string key = tune_key(b);
-  auto hit = g_tuned.find(key);
-  if (hit != g_tuned.end()) {
-    b->form = hit->second;
-    return VI_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    auto hit = g_tuned.find(key);
+    if (hit != g_tuned.end()) {
+      b->form = hit->second;
+      return VI_OK;
+    }
   }
   set_order(b);
   float best = 1e30f;
@@ -360,7 +365,10 @@ static int tune(vi_batch *b, cudaStream_t st) {
     }
   }
   b->form = choice;
-  g_tuned[key] = choice;
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    g_tuned[key] = choice;
+  }
   // tuning advanced the shots: put them back at rest
   return reset_state<T>(b, st);
 }
@@ -380,7 +388,10 @@ static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
   if (rc) return rc;
   const bool use_graph = (flags & VI_BATCH_NO_GRAPH) == 0;
   if (b->form < 0 || (flags & VI_BATCH_RETUNE)) {
-    if (flags & VI_BATCH_RETUNE) g_tuned.erase(tune_key(b));
+    if (flags & VI_BATCH_RETUNE) {
+      std::lock_guard<std::mutex> lk(g_tuned_mu);
+      g_tuned.erase(tune_key(b));
+    }
     if ((rc = tune<T>(b, st))) return rc;
     b->dirty = true;
   }

@@ -9,6 +9,7 @@
 //
 //   velocity: 64 x 16 tiles, 4-cell groups, 256 threads, 3 stages (FP32)
 //   stress:   64 x 8 tiles, 2-cell groups, 256 threads, 2 stages
+#include <atomic>
 #include <cudaTypedefs.h>
 
 #include <cstdint>
@@ -402,10 +403,10 @@ __global__ void __launch_bounds__(StressP<T, KIND, NSLS>::NT)
 
 // ------------------------------------------------------------------- host
 template <typename K>
-static int set_smem(K kern, int bytes, unsigned long long &done) {
+static int set_smem(K kern, int bytes, std::atomic<unsigned long long> &done) {
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 64 && !(done & (1ULL << dev))) {
+  if (dev < 64 && !(done.load() & (1ULL << dev))) {  // one bit per device set up (any thread)
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return cuda_check(e, "split pipeline smem attribute");
     done |= 1ULL << dev;
@@ -431,7 +432,7 @@ static int launch_stress_p(const StepArgs<T> &a, const FusedExtras<T> &x, const 
   if constexpr (!G::FITS) {
     return set_error(VI_ERR_ARG, "pipelined stress kernel does not fit shared memory");
   } else {
-    static unsigned long long done = 0;
+    static std::atomic<unsigned long long> done{0};
     int rc = set_smem(k_split_stress_p<T, KIND, NSLS>, G::BYTES, done);
     if (rc) return rc;
     const int grid = persistent_grid(k_split_stress_p<T, KIND, NSLS>, G::NT, G::BYTES, nsm, ntiles);
@@ -444,7 +445,7 @@ template <typename T>
 int launch_split_vel_p(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitPMaps &m,
                        int ntiles, int nsm, cudaStream_t st) {
   using G = VelP<T>;
-  static unsigned long long done = 0;
+  static std::atomic<unsigned long long> done{0};
   int rc = set_smem(k_split_vel_p<T>, G::BYTES, done);
   if (rc) return rc;
   const int grid = persistent_grid(k_split_vel_p<T>, G::NT, G::BYTES, nsm, ntiles);

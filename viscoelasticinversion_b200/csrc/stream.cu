@@ -525,7 +525,7 @@ static int launch_stream_k(const StepArgs<float> &a, const StreamExtras &x, cons
                            cudaStream_t st, bool pdl) {
   using LY = SLayout<KIND, NSLS>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
-  static int grid_per_dev[64] = {0};
+  static std::atomic<int> grid_per_dev[64];  // zero-initialised; any thread
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64) return set_error(VI_ERR_ARG, "device ordinal out of range");
@@ -535,11 +535,11 @@ static int launch_stream_k(const StepArgs<float> &a, const StreamExtras &x, cons
     int per = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stream<KIND, NSLS>, kNT, LY::BYTES);
     if (e != cudaSuccess) return cuda_check(e, "stream occupancy");
-    grid_per_dev[dev] = std::max(per, 1) * nsm;
+    grid_per_dev[dev].store(std::max(per, 1) * nsm);
     attr_set |= 1ULL << dev;
   }
   const long long units = (long long)x.nstrips * x.nchunks;
-  const int grid = (int)std::min<long long>(grid_per_dev[dev], units);
+  const int grid = (int)std::min<long long>(grid_per_dev[dev].load(), units);
   return cuda_check(launch_pdl(k_stream<KIND, NSLS>, dim3(grid), dim3(kNT), (size_t)LY::BYTES, st, pdl, a, x, m),
                     "stream launch");
 }
