@@ -84,3 +84,26 @@ def test_fwi_problem_checks_its_arguments():
     other = media.homogeneous_iso(nx=72, nz=48, nt=10, pml=6, nrec=4)
     with pytest.raises(ValueError, match="grid"):
         fwi.FWIProblem(w, [other], obs)
+
+
+def test_sensitivities_and_jvp_by_central_differences():
+    A = np.array([[1.0, 2.0, 0.0], [0.5, -1.0, 3.0]])
+    forward = lambda t: np.array([A @ t, np.sin(t).sum() * np.ones(2)])  # u: [2, 2]
+    theta = np.array([0.3, -0.7, 1.1])
+    sens = fwi.compute_sensitivities_forwardmode(forward, theta)
+    for i in range(3):
+        exact = np.array([A[:, i], np.cos(theta[i]) * np.ones(2)])
+        assert np.allclose(sens[i], exact, rtol=1e-8, atol=1e-9)
+    calls = []
+    batched = fwi.compute_sensitivities_forwardmode(
+        forward, theta, forward_batch=lambda ts: calls.append(len(ts)) or [forward(t) for t in ts])
+    assert calls == [6] and all(np.array_equal(a, b) for a, b in zip(sens, batched))
+    jvp = fwi.make_jvp_function(forward, theta)
+    v = np.array([1.0, -2.0, 0.5])
+    exact = np.array([A @ v, np.dot(np.cos(theta), v) * np.ones(2)])
+    assert np.allclose(jvp(v), exact, rtol=1e-8, atol=1e-9)
+    # with these, the optimizer's exact-Gram branch runs end to end
+    G = fwi.compute_gram_exact(sens)
+    assert np.allclose(G, G.T) and np.all(np.linalg.eigvalsh(G) > -1e-9)
+    Gs = fwi.compute_gram_stochastic(jvp, 3, 5, rng=np.random.default_rng(0))
+    assert Gs.shape == (3, 3) and np.allclose(Gs, Gs.T)

@@ -13,6 +13,9 @@ loss_fn(θ), grad_fn(θ) and sensitivity_fn(θ) (EnergyNaturalGradient.jl:
   sensitivity_fn = None the metric is the identity — the natural gradient
   is grad / (1 + regularization) — the one form that scales to gridded
   media (p = planes x nx x nz);
+* the sensitivity helpers (`compute_sensitivities_forwardmode`,
+  `make_jvp_function`) take central differences of a forward solve where
+  the reference takes ForwardDiff derivatives;
 * `FWIProblem` supplies loss_fn and grad_fn for seismic shots: the summed
   misfit J = 1/2 sum (d - obs)^2 and dJ/dθ by vi_gradient (the discrete
   adjoint in libvisco_b200.so), and `batch_loss` evaluates every trial
@@ -159,6 +162,43 @@ def optimize(state: OptimizationState, opt: EnergyNaturalGradientOptimizer, loss
             if abs(a - b) / (abs(b) + 1e-12) < 1e-10:
                 break
     return state
+
+
+# ---------------------------------------------------------------- sensitivities
+def compute_sensitivities_forwardmode(forward_solve, theta, step: float = 1e-6,
+                                      forward_batch=None) -> list:
+    """Wavefield sensitivities [∂θ1 u, ∂θ2 u, ...] for compute_gram_exact —
+    EnergyNaturalGradient.jl:337-356, which takes ForwardDiff derivatives
+    along each unit vector.  Here central differences of forward_solve
+    (θ -> u) with a step of `step` relative to max(1, |θi|); forward_batch,
+    if given, takes the list of 2p perturbed θ and returns their u in one
+    call (the GPU runs them as one batch)."""
+    theta = np.asarray(theta, dtype=np.float64).ravel()
+    hs = step * np.maximum(1.0, np.abs(theta))
+    trials = []
+    for i, h in enumerate(hs):
+        e = np.zeros_like(theta)
+        e[i] = h
+        trials += [theta + e, theta - e]
+    us = list(forward_batch(trials)) if forward_batch is not None else [forward_solve(t) for t in trials]
+    return [(np.asarray(us[2 * i], dtype=np.float64) - np.asarray(us[2 * i + 1], dtype=np.float64))
+            / (2.0 * h) for i, h in enumerate(hs)]
+
+
+def make_jvp_function(forward_solve, theta, step: float = 1e-6):
+    """v -> J v, the wavefield's directional derivative along v at θ, for
+    compute_gram_stochastic — EnergyNaturalGradient.jl:367-375 (ForwardDiff
+    there; a central difference of step `step` / max(|v|) here)."""
+    theta = np.asarray(theta, dtype=np.float64).ravel()
+
+    def jvp(v):
+        v = np.asarray(v, dtype=np.float64).ravel()
+        h = step / max(float(np.abs(v).max()), 1e-300)
+        up = np.asarray(forward_solve(theta + h * v), dtype=np.float64)
+        um = np.asarray(forward_solve(theta - h * v), dtype=np.float64)
+        return (up - um) / (2.0 * h)
+
+    return jvp
 
 
 # ---------------------------------------------------------------- seismic problem
