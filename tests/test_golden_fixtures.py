@@ -3,7 +3,8 @@ tests/golden/make_golden.py from the FP64 oracle).
 
 CPU: the workload builder still yields the fixture's medium and the oracle
 still yields its traces and final planes (1e-13 relative L2: the oracle is
-deterministic, but another host's compiler may round differently).
+deterministic, but another host's compiler may round differently); the
+oracle's FP32 twin meets the FP32 bar below.
 GPU: the default CUDA step, through the C ABI, against the fixture:
   FP32 ... 1e-5 relative L2 (traces, every final plane, memory-variable norms)
   FP64 ... 1e-10
@@ -42,6 +43,16 @@ def test_fixture_medium_and_oracle(oracle_lib, name):
     traces, st = oracle_lib.run(w, precision="f64")
     err = _errors(traces, st.v, st.s, st.m, g)
     assert max(err.values()) <= 1e-13, err
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fp32_oracle_matches_fixture(oracle_lib, name):
+    """The oracle's FP32 twin — the timed CPU baseline and reference arm —
+    meets the FP32 bar against the FP64 fixture, as the GPU path does."""
+    g = _fixture(name)
+    traces, st = oracle_lib.run(workload(name), precision="f32")
+    err = _errors(traces, st.v, st.s, st.m.astype(np.float64), g)
+    assert max(err.values()) <= TOL["f32"], err
 
 
 @pytest.mark.gpu
