@@ -51,6 +51,7 @@ def parse_args():
     p.add_argument("--precision", default="f32", choices=["f32", "f64"])
     p.add_argument("--variant", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-accuracy", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--batch-shots", type=int, default=64)
@@ -60,7 +61,6 @@ def parse_args():
     p.add_argument("--serve-requests", type=int, default=40)
     p.add_argument("--serve-explore", action="store_true",
                    help="time several slice lengths and both scheduling policies")
-    p.add_argument("--cpu-seconds", type=float, default=12.0)
     return p.parse_args()
 
 
@@ -150,20 +150,43 @@ def ncu_traffic(name: str):
     return None
 
 
-def cpu_baseline(w, seconds: float):
-    """Times the FP32 CPU oracle on the first steps of the workload."""
+# Both CPU legs (cpu_baseline and --impl reference) time the same bounded
+# sample: the first CPU_SAMPLE_STEPS steps of the workload (about 4 s of
+# FP32 oracle work on 16 host threads for 2048 x 1024).
+CPU_SAMPLE_STEPS = 200
+
+
+def host_cpu():
+    """The host's core count, CPU model and OpenMP thread setting."""
+    model = ""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model,
+            "OMP_NUM_THREADS": os.environ.get("OMP_NUM_THREADS", "unset (all cores)")}
+
+
+def cpu_sample(w):
+    """One timed FP32 oracle run of the bounded sample; (Gpt/s, steps, threads)."""
     import oracle
 
     oracle.build()
-    threads = oracle.num_threads()
-    t0 = time.perf_counter()
-    oracle.run(w, 2, precision="f32")
-    per = (time.perf_counter() - t0) / 2
-    n = int(max(4, min(400, w.nt, seconds / max(per, 1e-6))))
+    n = min(CPU_SAMPLE_STEPS, w.nt)
     t0 = time.perf_counter()
     oracle.run(w, n, precision="f32")
     dt = time.perf_counter() - t0
-    return {"value": w.nx * w.nz * n / dt / 1e9, "unit": "Gpt/s", "cores": threads, "kind": "port",
+    return w.nx * w.nz * n / dt / 1e9, n, oracle.num_threads()
+
+
+def cpu_baseline(w):
+    """Times the FP32 CPU oracle on the first steps of the workload."""
+    cpu_sample(w)  # warm-up (pages, thread pool)
+    value, n, threads = cpu_sample(w)
+    return {"value": value, "unit": "Gpt/s", "cores": threads, "kind": "port", **host_cpu(),
             "sample": f"first {n} of {w.nt} time steps of the {w.nx}x{w.nz} {w.kind.upper()} "
                       f"workload, FP32 CPU oracle, {threads} OpenMP threads"}
 
@@ -172,25 +195,17 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle
-
     w = workload(a)
-    oracle.build()
-    threads = oracle.num_threads()
-    t0 = time.perf_counter()
-    oracle.run(w, 2, precision="f32")
-    per = (time.perf_counter() - t0) / 2
-    # each bench step: a bounded sample of the solve (~8 s of CPU work)
-    n = int(max(2, min(200, w.nt, 8.0 / max(per, 1e-6))))
+    # each bench step: the same bounded sample of the solve as the
+    # cpu_baseline leg of the GPU arm
     for _ in range(a.warmup):
-        oracle.run(w, n, precision="f32")
-    times = []
+        cpu_sample(w)
+    rates = []
     for _ in range(a.steps):
-        t0 = time.perf_counter()
-        oracle.run(w, n, precision="f32")
-        times.append(time.perf_counter() - t0)
-    ms = 1e3 * sum(times) / len(times)
-    value = w.nx * w.nz * n / (ms / 1e3) / 1e9
+        value, n, threads = cpu_sample(w)
+        rates.append(value)
+    value = len(rates) / sum(1.0 / r for r in rates)  # total points / total time
+    ms = w.nx * w.nz * n / value / 1e6
     sample = (f"first {n} of {w.nt} time steps of the {w.nx}x{w.nz} {w.kind.upper()} workload per "
               f"step; FP32 CPU restatement of the reference step (the Julia reference does not run "
               f"here), {threads} OpenMP threads")
@@ -198,9 +213,10 @@ def run_reference(a):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gpt/s", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(a), "nx": w.nx, "nz": w.nz, "nt_sampled": n},
+        "config": {"workload": workload_name(a), "nx": w.nx, "nz": w.nz, "nt": w.nt, "nt_sampled": n,
+                   "nsls": w.nsls, "medium": w.kind},
         "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, **host_cpu()},
         "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -210,11 +226,12 @@ SMALL_GRIDS = ((256, 256), (384, 256), (512, 256))
 
 def measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=False):
     """Shots/s of the batched TTI gather (64 shots, grids from {512²,
-    1024x512, 1536x768, 2048x1024}, nt in [1500, 4000], one CUDA graph)
-    against the plain path (the kernel form the tuner picked, one shot
-    after the other, launched step by step, no graph).  small: the same
-    with grids from {256², 384x256, 512x256}, where one shot does not fill
-    the GPU.  Each rank runs its own gather."""
+    1024x512, 1536x768, 2048x1024}, nt in [1500, 4000], the kernel form the
+    tuner picks, one CUDA graph) against the plain path: the default split
+    pair (vi_step kernel variant 5), one shot after the other, launched
+    step by step, no graph.  small: the same with grids from {256²,
+    384x256, 512x256}, where one shot does not fill the GPU.  Each rank
+    runs its own gather."""
     import torch
 
     from viscoelasticinversion_b200 import StepPlan, media
@@ -229,7 +246,7 @@ def measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=False):
     b.run()  # tunes the kernel form, captures the graph, runs once
     b.reset()
     form = b.status()
-    variant = {"per-shot": 0, "split": 5, "two-stage": 3, "one-stage": 4}[form]
+    variant = 5  # plain: the default single-shot split pair, whatever the tuner picked
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -426,6 +443,51 @@ def measure_gradient(a, dev):
             "grad_finite": bool(torch.isfinite(g).all().item())}
 
 
+def measure_accuracy(a, w, plan, med, st, traces, dev):
+    """Relative L2 error of the timed solve (its traces and final fields,
+    left by the last timed step) against the same solve in FP64 on the GPU,
+    over the full step count.  The FP64 kernels are held to the FP64 oracle
+    within 1e-10 on this workload over all its steps by
+    tests/test_gpu_accuracy.py, so these errors are those against the oracle
+    to within 1e-10."""
+    import numpy as np
+    import torch
+
+    from viscoelasticinversion_b200 import StepPlan
+
+    if a.precision == "f64":
+        return None
+    ref = StepPlan.for_workload(w, "f64", device=dev.index)
+    med64 = ref.medium_to_device(w.medium)
+    st64 = ref.zeros_state()
+    wav64 = torch.as_tensor(w.wavelets, dtype=torch.float64, device=dev).contiguous()
+    tr64 = torch.zeros(2, len(w.receivers), w.nt, dtype=torch.float64, device=dev)
+    ref.reset()
+    ref.step(med64, st64, nsteps=w.nt, sources=w.sources, wavelets=wav64, receivers=w.receivers,
+             traces=tr64, variant=a.variant)
+    ref.status()
+
+    def rel(x, y):
+        x = x.double()
+        n = torch.linalg.vector_norm(y).item()
+        return torch.linalg.vector_norm(x - y).item() / (n if n > 0 else 1.0)
+
+    out = {"reference": "the same solve in FP64 on the GPU (FP64 kernels = FP64 oracle to 1e-10 over "
+                        "all steps of this workload, tests/test_gpu_accuracy.py)",
+           "nt": w.nt, "bar": 1e-5, "traces": rel(traces, tr64),
+           "vx": rel(st["v"][0], st64["v"][0]), "vz": rel(st["v"][1], st64["v"][1]),
+           "sxx": rel(st["s"][0], st64["s"][0]), "szz": rel(st["s"][1], st64["s"][1]),
+           "sxz": rel(st["s"][2], st64["s"][2])}
+    if w.nsls:
+        m32, m64 = st["m"].reshape(3 * w.nsls, -1), st64["m"].reshape(3 * w.nsls, -1)
+        out["m"] = rel(m32, m64)
+        out["m_plane_max"] = max(rel(m32[q], m64[q]) for q in range(3 * w.nsls))
+    out["max"] = max(v for k, v in out.items() if isinstance(v, float) and k != "bar")
+    out["within_bar"] = out["max"] <= 1e-5
+    ref.close()
+    return out
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -535,6 +597,9 @@ def run_ours(a):
         "clocks": clk,
     }
 
+    if not a.no_accuracy:
+        out["accuracy"] = measure_accuracy(a, w, plan, med, st, traces, dev)
+
     if not a.no_e2e:
         # end to end through vi_forward_host with pinned host buffers
         npdt = np.float64 if a.precision == "f64" else np.float32
@@ -579,7 +644,7 @@ def run_ours(a):
                                  ("shortest-first-4096", (4096, 64, "shortest-first", 2))]
         out["serving"] = measure_serving(a, dev)
     if rank == 0 and world == 1 and not a.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(w, a.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
         print(json.dumps(out), flush=True)
     plan.close()

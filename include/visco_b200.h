@@ -57,6 +57,13 @@ extern "C" {
 
 #define VI_F32 0
 #define VI_F64 1
+/* FP32 fields whose split-pair stress update is compensated: each cell's
+ * rounding error of sxx, szz and sxz is kept in a bfloat16 residue plane
+ * of the plan and folded into the next update (an error-free two-sum), so
+ * the float stresses do not drift over long runs.  Costs 12 bytes per cell
+ * per step (about 13 % of the 2048 x 1024 VTI step); kernel variants 0, 5
+ * and 8 only (the others return VI_ERR_ARG). */
+#define VI_F32C 2
 
 /* source kinds */
 #define VI_SRC_EXPLOSIVE 0  /* sxx, szz += dt*amp*w(t) */
@@ -70,9 +77,15 @@ typedef struct vi_config {
   int32_t nx, nz;
   double dx, dz, dt;
   int32_t medium;          /* VI_MEDIUM_* */
-  int32_t precision;       /* VI_F32 / VI_F64 */
+  int32_t precision;       /* VI_F32 / VI_F64 / VI_F32C */
   int32_t nsls;            /* 0..VI_MAX_SLS */
-  int32_t free_surface;    /* 1: stress-imaging free surface at row VI_HALF */
+  int32_t free_surface;    /* 0 none (top CPML allowed); 1 stress-imaging
+                              free surface at row VI_HALF (CPML.jl:366-393);
+                              2 H-AFDA free surface at row VI_HALF: the z
+                              derivatives whose stencil would reach above it
+                              are one-sided (free-surface-kernels.jl:16-213,
+                              Stencil.jl:52-105), nothing is written above
+                              it; kernel variants 0, 1, 5 and 8 only */
   double tau_sls[VI_MAX_SLS]; /* relaxation times tau_n of the mechanisms */
   /* CPML */
   int32_t pml_thickness;   /* cells, counted from the array edge */
@@ -142,13 +155,19 @@ const char *vi_last_error(void);
  * (Parameters.jl:47-86) for the leapfrog path. */
 int vi_plan_create(const vi_config *cfg, vi_plan **out);
 int vi_plan_destroy(vi_plan *plan);
-/* Zeroes the plan's CPML memory variables (CPMLMemory, CPML.jl:246-263). */
+/* Zeroes the plan's CPML memory variables (CPMLMemory, CPML.jl:246-263)
+ * and, for VI_F32C plans, the stress rounding residues (see VI_F32C).  Call
+ * it whenever the caller resets or replaces the fields between calls. */
 int vi_plan_reset(vi_plan *plan, void *stream);
 /* Bytes of device memory the plan holds. */
 int vi_plan_workspace_bytes(const vi_plan *plan, int64_t *bytes);
 /* Synchronizes `stream` and reports (then clears) the plan's device error
- * word: VI_ERR_TIMEOUT when a bounded in-kernel wait gave up.  Kernels never
- * trap; this is how a device-side failure reaches the caller. */
+ * word: VI_ERR_TIMEOUT when a bounded in-kernel wait gave up,
+ * VI_ERR_NONFINITE when a stress value came out NaN or infinite (a
+ * non-finite medium or state, or an unstable run; the split pair checks
+ * every step in its stress pass, the other paths once at the end of each
+ * vi_step call).  Kernels never trap; this is how a device-side failure
+ * reaches the caller. */
 int vi_plan_status(vi_plan *plan, void *stream);
 /* Which kernel the last vi_step ran: 1 plain, 2 fused, 3 fused TMA-staged,
  * 4 fused TMA-staged single-stage, 5 split velocity/stress pair, 6 split
@@ -178,7 +197,10 @@ int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
  * strips with TMA row rings, one launch per step),
  * 8 = the split pair of 5 with its velocity pass reading the stress taps
  * straight through L1 instead of TMA boxes.
- * Variants 3-8 return VI_ERR_ARG when not eligible. */
+ * Variants 3-8 return VI_ERR_ARG when not eligible.
+ * VI_F32C plans (split pair only) keep the stresses' rounding residues as
+ * plan state, continued across calls like the CPML memory: vi_plan_reset
+ * zeroes them. */
 int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);
@@ -190,10 +212,14 @@ int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
  * that must not call cudaMalloc/cudaFree mid-run (a serving process sharing
  * the GPU, whose allocations would synchronize it; a fully reserved HBM
  * pool).  Limit: 6*nx*nz reals of the plan's precision plus the lists
- * (<= 256 sources) must fit, else VI_ERR_ARG.  The first call on a device
- * looks up the array's address; make it before any stream capture.  Each
- * call clears the strain planes first.  Calls overlapping in time on one
- * device race on the array: serialize them. */
+ * (<= 256 sources; each of the three blocks rounded up to 256 bytes) must
+ * fit in VI_NOALLOC_SCRATCH_BYTES, else VI_ERR_ARG.  Every call looks up
+ * the array's address in the current context; the first call on a device
+ * loads the module that holds it, so make that first call before any
+ * stream capture.  With sources or receivers (nsrc > 0 or nrec > 0) the
+ * call blocks the host thread until their lists are staged on the device.
+ * Each call clears the strain planes first.  Calls overlapping in time on
+ * one device race on the array: serialize them. */
 #define VI_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
 int vi_step_noalloc(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
                     const vi_shot *shot, int32_t it0, int32_t nsteps, void *stream);
@@ -249,7 +275,10 @@ int vi_batch_status(vi_batch *batch, void *stream, int32_t *kernel_form);
  * ([2][nrec][nt], plan precision).  grad_dev (8 planes of nx*nz, FP64) gets
  * dJ/d(rho, c11, c13, c15, c33, c35, c55, tau) in vi_medium's order; for
  * ISO media the c13 plane holds dJ/dlambda and the c55 plane dJ/dmu (the
- * others zero).  ISO and VTI media; TTI returns VI_ERR_ARG.  The adjoint
+ * others zero).  ISO, VTI and TTI media (TTI fills all eight planes: the
+ * tilted law of custom_solver/Model.jl:59-108 transposed, its 4-point means
+ * of C15/C35/C55 and of the effective rates and the surface relation with
+ * C35 included); the H-AFDA surface returns VI_ERR_ARG.  The adjoint
  * is the exact transpose of the plain in-place step (kernel variant 1),
  * with the state checkpointed every checkpoint_every steps (<= 0: ceil
  * sqrt(nt)) in the plan's workspace.  accumulate != 0 adds into grad_dev
@@ -276,6 +305,17 @@ int vi_gradient_velocity(int32_t medium, int64_t np, const double *grad8, const 
  * planes of np cells; asynchronous on `stream`. */
 int vi_gradient_thomsen(int64_t np, const double *grad8, const double *vp, const double *vs,
                         const double *rho, const double *delta, double *out2, void *stream);
+
+/* TTI: from the same grad planes to out7 = [dJ/dvp, dJ/dvs, dJ/drho,
+ * dJ/d(1/Q), dJ/d(epsilon), dJ/d(delta), dJ/d(theta)] through the map of
+ * vi_medium_from_velocity (Thomsen's VTI law, Models.jl:27-52 and
+ * custom_solver/Model.jl:12-16, tilted by theta with the 2D Bond rotation);
+ * dJ/drho at fixed velocities includes the buoyancy term.  eps, delta,
+ * theta NULL mean 0.  gamma enters only SH motion: no 2D P-SV gradient.
+ * FP64 device planes of np cells; asynchronous on `stream`. */
+int vi_gradient_tti(int64_t np, const double *grad8, const double *vp, const double *vs, const double *rho,
+                    const double *eps, const double *delta, const double *theta, double tau_scale,
+                    double *out7, void *stream);
 
 /* ---- medium parameterisation ------------------------------------------ */
 /* Writes the medium planes the step reads from FP64 parameter planes of np

@@ -56,6 +56,8 @@ def lib():
         h.or_stencil8.restype = None
         h.or_stencil8.argtypes = [C.POINTER(C.c_double)]
         h.or_num_threads.restype = C.c_int
+        h.or_afda_weights.restype = None
+        h.or_afda_weights.argtypes = [C.POINTER(C.c_double)]
         _lib = h
     return _lib
 
@@ -69,7 +71,7 @@ def make_config(w, precision: str = "f64") -> ViConfig:
     c.nsls = w.nsls
     for n, t in enumerate(w.taus):
         c.tau_sls[n] = float(t)
-    c.free_surface = int(w.free_surface)
+    c.free_surface = 2 if w.free_surface == 2 else int(bool(w.free_surface))
     c.pml_thickness = w.pml
     c.pml_left = c.pml_right = c.pml_bottom = 1
     c.pml_top = 0 if w.free_surface else 1
@@ -156,6 +158,13 @@ def ricker(f: float, t: float) -> float:
 def stencil8() -> np.ndarray:
     out = np.zeros(4)
     lib().or_stencil8(out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def afda_weights() -> np.ndarray:
+    """The oracle's H-AFDA one-sided weights w[op, q, m] (unit spacing)."""
+    out = np.zeros((4, 4, 5))
+    lib().or_afda_weights(out.ctypes.data_as(C.POINTER(C.c_double)))
     return out
 
 

@@ -14,6 +14,8 @@
  *   CPML profiles and a/b coefficients ............... src/sciml_solver/CPML.jl:55-61,91-102,109-189
  *   CPML derivative correction du/kappa + psi ........ src/sciml_solver/CPML.jl:291-308
  *   stress imaging free surface ...................... src/sciml_solver/CPML.jl:366-393
+ *   H-AFDA free surface (one-sided z derivatives) ..... src/free-surface-kernels.jl:16-213,
+ *                                                       src/common/Stencil.jl:52-105
  *   tau_zz = 0 relation at the surface ............... src/free-surface-kernels.jl:84-95,106,116
  *   Ricker wavelet ................................... src/sciml_solver/Source.jl:3-5
  *   source added before buoyancy scaling ............. src/sciml_solver/ViscoelasticProblem.jl:162-171
@@ -47,6 +49,82 @@ void or_stencil8(double *D) {
 double or_ricker(double f, double t) {
   const double x = M_PI * f * t;
   return (1.0 - 2.0 * x * x) * exp(-x * x);
+}
+
+/* Weights w[0..n-1] of the first derivative at x0 from samples at x[0..n-1]
+ * (n <= 8): the conditions sum_k w_k (x_k - x0)^l / l! = [l == 1], l < n,
+ * the Vandermonde system Stencil.jl:_stencil solves in rationals (its
+ * lines 9-14), here by Gaussian elimination with partial pivoting. */
+static void fd_weights(const double *x, int n, double x0, double *w) {
+  double A[8][9];
+  for (int l = 0; l < n; ++l) {
+    double fact = 1.0;
+    for (int q = 2; q <= l; ++q) fact *= q;
+    for (int k = 0; k < n; ++k) A[l][k] = pow(x[k] - x0, l) / fact;
+    A[l][n] = l == 1 ? 1.0 : 0.0;
+  }
+  for (int c = 0; c < n; ++c) {
+    int p = c;
+    for (int r = c + 1; r < n; ++r)
+      if (fabs(A[r][c]) > fabs(A[p][c])) p = r;
+    for (int k = 0; k <= n; ++k) {
+      const double t = A[c][k];
+      A[c][k] = A[p][k];
+      A[p][k] = t;
+    }
+    for (int r = 0; r < n; ++r)
+      if (r != c && A[r][c] != 0.0) {
+        const double f = A[r][c] / A[c][c];
+        for (int k = c; k <= n; ++k) A[r][k] -= f * A[c][k];
+      }
+  }
+  for (int k = 0; k < n; ++k) w[k] = A[k][n] / A[k][k];
+}
+
+/* H-AFDA free surface (Kristek, Moczo & Archuleta 2002; the reference's
+ * FreeSurfaceStencil, Stencil.jl:52-105, and its kernels,
+ * free-surface-kernels.jl:16-213): the surface z = 0 lies on the row of
+ * sxx, szz and vx (row VI_HALF); szz(0) = 0 and sxz(0) = 0 there; nothing
+ * lives above it.  The z derivatives whose 8th-order staggered stencil
+ * would reach above the surface use adjusted one-sided approximations of
+ * AFDA_N = 5 samples (plus the zero boundary value where there is one):
+ *   0  d(sxz)/dz at vx rows z = q h (q = 0..3): samples sxz at (m + 1/2) h,
+ *      m = 0..4, and sxz(0) = 0;
+ *   1  d(szz)/dz at vz rows z = (q + 1/2) h (q = 0..2): samples szz at
+ *      m h, m = 1..5, and szz(0) = 0;
+ *   2  d(vz)/dz at szz rows z = q h (q = 1..3): samples vz at (m + 1/2) h,
+ *      m = 0..4 (on the surface row the tau_zz = 0 relation gives it);
+ *   3  d(vx)/dz at sxz rows z = (q + 1/2) h (q = 0..2): samples vx at m h,
+ *      m = 0..4.
+ * w[op][q][m] (unit spacing) multiplies the sample of row VI_HALF + m
+ * (op 1: row VI_HALF + 1 + m).  The reference builds these one-sided
+ * approximations with as many samples as the interior stencil (8); with 8
+ * the semi-discrete operator has growing modes (eigenvalues with real
+ * part 0.4 c/h in a 1D half-space), with 5 it has none, so 5 are used. */
+void or_afda_weights(double w[4][4][AFDA_N]) {
+  double x[AFDA_N + 1], t[AFDA_N + 1];
+  memset(w, 0, sizeof(double) * 4 * 4 * AFDA_N);
+  for (int q = 0; q < 4; ++q) { /* op 0 */
+    x[0] = 0.0;
+    for (int m = 0; m < AFDA_N; ++m) x[m + 1] = m + 0.5;
+    fd_weights(x, AFDA_N + 1, (double)q, t);
+    for (int m = 0; m < AFDA_N; ++m) w[0][q][m] = t[m + 1];
+  }
+  for (int q = 0; q < 3; ++q) { /* op 1 */
+    for (int m = 0; m <= AFDA_N; ++m) x[m] = m;
+    fd_weights(x, AFDA_N + 1, q + 0.5, t);
+    for (int m = 0; m < AFDA_N; ++m) w[1][q][m] = t[m + 1];
+  }
+  for (int q = 1; q < 4; ++q) { /* op 2 */
+    for (int m = 0; m < AFDA_N; ++m) x[m] = m + 0.5;
+    fd_weights(x, AFDA_N, (double)q, t);
+    for (int m = 0; m < AFDA_N; ++m) w[2][q][m] = t[m];
+  }
+  for (int q = 0; q < 3; ++q) { /* op 3 */
+    for (int m = 0; m < AFDA_N; ++m) x[m] = m;
+    fd_weights(x, AFDA_N, q + 0.5, t);
+    for (int m = 0; m < AFDA_N; ++m) w[3][q][m] = t[m];
+  }
 }
 
 int or_num_threads(void) {

@@ -53,6 +53,12 @@ double or_ricker(double f, double t);
 /* The 8th-order staggered half-stencil D[0..3] (unit spacing). */
 void or_stencil8(double *D);
 
+/* H-AFDA free surface (vi_config.free_surface = 2): unit-spacing weights of
+ * the adjusted one-sided z derivatives near the surface, w[op][q][m]
+ * (see visco_oracle.c for the operators, rows and samples). */
+#define AFDA_N 5
+void or_afda_weights(double w[4][4][AFDA_N]);
+
 /* Number of OpenMP threads the oracle uses. */
 int or_num_threads(void);
 

@@ -82,6 +82,13 @@ def _vti(nt=300):
                          f0=25.0)
 
 
+def _tti(nt=300, fs=True):
+    # the C3-style tilted medium at test size: every stiffness plane of the
+    # rotated law (C15 and C35 included) is non-zero
+    return media.layered(nx=128, nz=96, nt=nt, kind="tti", pml=12, nrec=16, nlayers=4, seed=6,
+                         f0=25.0, free_surface=fs)
+
+
 def _bump(w, rel=0.25):
     """Positive Gaussian bump between the source and the receiver line."""
     (si, sj), (ri, rj) = w.sources[0][:2], w.receivers[len(w.receivers) // 2]
@@ -112,31 +119,36 @@ def _directional(oracle_lib, w, obs, g, planes, scale=1e-4):
             assert abs(fd - an) <= tol * abs(an), (k, name, fd, an)
 
 
-@pytest.mark.parametrize("case", ["iso", "iso-force-nosurface", "vti"])
+@pytest.mark.parametrize("case", ["iso", "iso-force-nosurface", "vti", "tti", "tti-nosurface"])
 def test_gradient_matches_oracle_finite_differences(oracle_lib, case):
     if case == "vti":
         w = _vti()
+    elif case.startswith("tti"):
+        w = _tti(fs=case == "tti")
     else:
         w = _iso(fs=case == "iso", force="force" in case)
     obs, _ = oracle_lib.run(_truth(w), precision="f64")
     J, g = _gpu_gradient(w, obs)
     J0 = _oracle_J(oracle_lib, w, obs)
     assert abs(J - J0) <= 1e-10 * J0, (J, J0)
-    planes = ["rho", "c13", "c55", "tau"] if w.kind == "iso" else ["rho", "c11", "c13", "c33", "c55", "tau"]
+    planes = {"iso": ["rho", "c13", "c55", "tau"], "vti": ["rho", "c11", "c13", "c33", "c55", "tau"],
+              "tti": list(GRADIENT_PLANES)}[w.kind]
     _directional(oracle_lib, w, obs, g, planes)
     for k in GRADIENT_PLANES:
         if k not in planes:
             assert not np.any(g[GRADIENT_PLANES.index(k)]), k
 
 
-def test_gradient_single_cells(oracle_lib):
-    w = _iso()
+@pytest.mark.parametrize("kind", ["iso", "tti"])
+def test_gradient_single_cells(oracle_lib, kind):
+    w = _iso() if kind == "iso" else _tti()
     obs, _ = oracle_lib.run(_truth(w), precision="f64")
     _, g = _gpu_gradient(w, obs)
     rng = np.random.default_rng(20)
     lo = w.pml + 4
+    names = ("c55", "c13") if kind == "iso" else ("c15", "c35", "c55", "c13", "c11", "c33")
     for n in range(20):
-        k = ("c55", "c13")[n % 2]
+        k = names[n % len(names)]
         gi = g[GRADIENT_PLANES.index(k)]
         i, j = int(rng.integers(lo, w.nx - lo)), int(rng.integers(5, w.nz - lo))
         h = 1e-4 * w.medium[k][j, i]
@@ -147,8 +159,9 @@ def test_gradient_single_cells(oracle_lib):
         assert abs(fd - gi[j, i]) <= CELL_TOL * abs(gi[j, i]) + 1e-7 * np.abs(gi).max(), (k, i, j, fd, gi[j, i])
 
 
-def test_checkpoint_interval_and_precision(oracle_lib):
-    w = _vti(nt=200)
+@pytest.mark.parametrize("kind", ["vti", "tti"])
+def test_checkpoint_interval_and_precision(oracle_lib, kind):
+    w = _vti(nt=200) if kind == "vti" else _tti(nt=200)
     obs, _ = oracle_lib.run(_truth(w), precision="f64")
     J0, g0 = _gpu_gradient(w, obs, K=0)
     for K in (1, 7, w.nt):
@@ -156,7 +169,8 @@ def test_checkpoint_interval_and_precision(oracle_lib):
         assert J == J0 and np.array_equal(g, g0), K
     J32, g32 = _gpu_gradient(w, obs, precision="f32")
     assert abs(J32 - J0) <= 1e-4 * J0
-    for k in ("rho", "c11", "c13", "c33", "c55", "tau"):
+    planes = ("rho", "c11", "c13", "c33", "c55", "tau") + (("c15", "c35") if kind == "tti" else ())
+    for k in planes:
         i = GRADIENT_PLANES.index(k)
         assert rel_l2(g32[i], g0[i]) <= 1e-3, (k, rel_l2(g32[i], g0[i]))
 
@@ -268,3 +282,59 @@ def test_autograd_function(oracle_lib):
     gv = velocity_gradient("iso", g0, vp.detach(), vs, rho)
     assert rel_l2(vp.grad.cpu().numpy(), gv[0].cpu().numpy()) <= 1e-12
     plan.close()
+
+
+def test_tti_parameter_chain_rule(oracle_lib):
+    """dJ/d(vp, vs, rho, 1/Q, epsilon, delta, theta) of a TTI medium
+    (vi_gradient_tti): against central differences of the host map (Thomsen
+    law tilted by media.bond_rotate) contracted with the stiffness gradient,
+    and for epsilon and theta against central differences of the oracle's
+    misfit along the gradient."""
+    from viscoelasticinversion_b200.gradient import TTI_PARAMETERS, tti_gradient
+
+    w = _tti()
+    qf = media.q_fit(*w.meta["band"], w.nsls)
+    fields = dict(w.meta["fields"])
+    fields["theta"] = w.meta["theta"]
+
+    def planes(f):
+        vti = media.medium_from_velocity("vti", f["vp"], f["vs"], f["rho"], f["eps"], f["delta"], f["Q"], qf)
+        n11, n13, n15, n33, n35, n55 = media.bond_rotate(vti["c11"], vti["c13"], vti["c33"], vti["c55"],
+                                                         f["theta"])
+        return {"rho": vti["rho"], "c11": n11, "c13": n13, "c15": n15, "c33": n33, "c35": n35, "c55": n55,
+                "tau": vti["tau"]}
+
+    w = _with(w, **planes(fields))
+    obs, _ = oracle_lib.run(_truth(w), precision="f64")
+    _, g = _gpu_gradient(w, obs)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    gt = tti_gradient(dev(g), dev(fields["vp"]), dev(fields["vs"]), dev(fields["rho"]), dev(fields["eps"]),
+                      dev(fields["delta"]), dev(fields["theta"]), tau_scale=w.nsls / qf.Kbar).cpu().numpy()
+    # the host map's derivative, parameter by parameter, contracted with g
+    for n, name in enumerate(TTI_PARAMETERS):
+        base = 1.0 / fields["Q"] if name == "qinv" else fields[name]
+        h = 1e-6 * max(np.abs(base).max(), 1e-3)
+
+        def pl(sign):
+            f = dict(fields)
+            if name == "qinv":
+                f["Q"] = 1.0 / (base + sign * h)
+            else:
+                f[name] = base + sign * h
+            return planes(f)
+
+        pp, pm = pl(1.0), pl(-1.0)
+        ref = sum(g[GRADIENT_PLANES.index(k)] * (pp[k] - pm[k]) / (2 * h) for k in GRADIENT_PLANES)
+        assert rel_l2(gt[n], ref) <= 1e-6, (name, rel_l2(gt[n], ref))
+    for name in ("eps", "theta"):
+        n = TTI_PARAMETERS.index(name)
+        d = 1e-4 * gt[n] / np.abs(gt[n]).max()
+
+        def J_of(hh):
+            f = dict(fields)
+            f[name] = fields[name] + hh * d
+            return _oracle_J(oracle_lib, _with(w, **planes(f)), obs)
+
+        fd = _richardson(J_of)
+        an = float(np.sum(gt[n] * d))
+        assert abs(fd - an) <= FD_REL_TOL * abs(an), (name, fd, an)

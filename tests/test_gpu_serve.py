@@ -135,10 +135,13 @@ def test_budget_admission():
 
 
 def test_failed_request_reports_error():
+    import dataclasses
+
     w = media.layered(nx=128, nz=64, nt=40, kind="tti", seed=1, pml=8, nrec=4)
+    bad = dataclasses.replace(w, free_surface=2)  # the adjoint covers the imaging surface only
     srv = Server()
-    t = srv.submit_gradient(w, np.zeros((2, len(w.receivers), w.nt)), "f64")  # TTI has no gradient
-    with pytest.raises(ViError, match="TTI"):
+    t = srv.submit_gradient(bad, np.zeros((2, len(w.receivers), w.nt)), "f64")
+    with pytest.raises(ViError, match="H-AFDA"):
         srv.wait(t, 60.0)
     with pytest.raises(ViError):
         srv.poll(t)

@@ -1,16 +1,17 @@
 """vi_step_noalloc (static device scratch, no allocation) against vi_step's
-plain path: two calls in a row, each compared with the allocating entry
-point's output.  Collected last on purpose."""
+plain path: two calls in a row, each compared bit for bit with the
+allocating entry point's output, with no device memory taken by either
+call.  Collected last on purpose: callers that cannot allocate (a process
+sharing the GPU with a serving loop, a fully reserved memory pool) depend
+on this path, and every other test has run before it."""
 import ctypes as C
 
-import numpy as np
 import pytest
 import torch
 
 from viscoelasticinversion_b200 import StepPlan, media
 from viscoelasticinversion_b200._abi import ViError, check, lib
 from viscoelasticinversion_b200.solver import _stream_handle
-from tests.helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -27,40 +28,63 @@ def _noalloc(plan, med, st, it0, n, w, wav, traces):
 
 @pytest.mark.parametrize("kind,precision", [("iso", "f32"), ("tti", "f32"), ("vti", "f64")])
 def test_noalloc_matches_plain_step_two_calls(kind, precision):
+    """Two vi_step_noalloc calls in a row on a fresh plan that has never run
+    vi_step, each bitwise equal to vi_step's plain path (the same kernels)
+    after the same steps, with the plan's device bytes and the device's
+    free memory unchanged across both calls."""
     if kind == "iso":
         w = media.homogeneous_iso(nx=96, nz=80, nt=120, pml=12, nrec=16)
     else:
         w = media.layered(nx=128, nz=96, nt=120, kind=kind, pml=12, nrec=16, nlayers=4)
-    plan = StepPlan.for_workload(w, precision)
-    med = plan.medium_to_device(w.medium)
-    wav = torch.as_tensor(w.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
-    tol = 1e-12 if precision == "f64" else 1e-6
-    ref_st, new_st = plan.zeros_state(), plan.zeros_state()
-    ref_tr = torch.zeros(2, len(w.receivers), w.nt, dtype=plan.dtype, device=plan.device)
-    new_tr = torch.zeros_like(ref_tr)
-    # reference: the allocating plain path, in the same two chunks
-    plan.reset()
-    it = 0
-    ref_chunks = []
-    for n in (70, 50):
-        plan.step(med, ref_st, nsteps=n, it0=it, sources=w.sources, wavelets=wav,
-                  receivers=w.receivers, traces=ref_tr, variant=1)
-        plan.status()
+    chunks = (70, 50)
+    # reference: the allocating plain path on its own plan, in the same chunks
+    ref = StepPlan.for_workload(w, precision)
+    med = ref.medium_to_device(w.medium)
+    wav = torch.as_tensor(w.wavelets, dtype=ref.dtype, device=ref.device).contiguous()
+    ref_st = ref.zeros_state()
+    ref_tr = torch.zeros(2, len(w.receivers), w.nt, dtype=ref.dtype, device=ref.device)
+    ref.reset()
+    it, ref_chunks = 0, []
+    for n in chunks:
+        ref.step(med, ref_st, nsteps=n, it0=it, sources=w.sources, wavelets=wav,
+                 receivers=w.receivers, traces=ref_tr, variant=1)
+        ref.status()
         ref_chunks.append(({k: v.clone() for k, v in ref_st.items()}, ref_tr.clone()))
         it += n
+    # one throw-away call on the reference plan loads the module that holds
+    # the static array and the plain kernels (lazy loading maps them on first
+    # use), so the measured calls below start from a loaded library
+    warm_st = ref.zeros_state()
+    _noalloc(ref, med, warm_st, 0, 2, w, wav, torch.zeros_like(ref_tr))
+    ref.status()
+    # the plan under test has never run vi_step: nothing was grown on it
+    plan = StepPlan.for_workload(w, precision)
+    new_st = plan.zeros_state()
+    new_tr = torch.zeros_like(ref_tr)
+    first = ({k: torch.empty_like(v) for k, v in new_st.items()}, torch.empty_like(new_tr))
+    torch.cuda.synchronize()
+    bytes0 = plan.workspace_bytes()
+    free0 = torch.cuda.mem_get_info()[0]
     plan.reset()
     it = 0
-    for k, n in enumerate((70, 50)):  # two calls in a row
+    for k, n in enumerate(chunks):  # two calls in a row
         _noalloc(plan, med, new_st, it, n, w, wav, new_tr)
         plan.status()
-        st_ref, tr_ref = ref_chunks[k]
-        assert rel_l2(new_tr.double().cpu().numpy(), tr_ref.double().cpu().numpy()) <= tol
-        for name in ("v", "s", "m"):
-            assert rel_l2(new_st[name].double().cpu().numpy(),
-                          st_ref[name].double().cpu().numpy()) <= tol, (k, name)
+        if k == 0:  # copy into buffers allocated before the measurement
+            for name, t in new_st.items():
+                first[0][name].copy_(t)
+            first[1].copy_(new_tr)
         it += n
-    assert np.abs(new_tr.double().cpu().numpy()).max() > 0
+    torch.cuda.synchronize()
+    assert plan.workspace_bytes() == bytes0
+    assert torch.cuda.mem_get_info()[0] == free0
+    for (st_got, tr_got), (st_ref, tr_ref) in zip((first, (new_st, new_tr)), ref_chunks):
+        assert torch.equal(tr_got, tr_ref)
+        for name in ("v", "s", "m"):
+            assert torch.equal(st_got[name], st_ref[name]), name
+    assert new_tr.abs().max().item() > 0
     plan.close()
+    ref.close()
 
 
 def test_noalloc_rejects_oversize_grid():

@@ -29,6 +29,8 @@ VI_MEDIUM_VTI = 1
 VI_MEDIUM_TTI = 2
 VI_F32 = 0
 VI_F64 = 1
+VI_F32C = 2  # FP32 fields, split-pair stress update compensated (residues in the plan)
+PRECISIONS = {"f32": VI_F32, "f64": VI_F64, "f32c": VI_F32C}
 VI_SRC_EXPLOSIVE = 0
 VI_SRC_FORCE_X = 1
 VI_SRC_FORCE_Z = 2
@@ -157,6 +159,9 @@ _SIGNATURES = [
                                        C.c_void_p, C.c_void_p]),
     ("vi_gradient_thomsen", C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("vi_gradient_tti", C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                  C.c_void_p]),
     ("vi_medium_from_velocity", C.c_int, [C.c_int32, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_double, C.POINTER(ViMedium), C.c_void_p]),

@@ -48,6 +48,7 @@ struct AdjArgs {
   T Dx[4], Dz[4];
   T a1[VI_MAX_SLS], a2[VI_MAX_SLS];
   const T *rho, *c11, *c13, *c33, *c55, *tau;
+  const T *c15, *c35;  // TTI couplings
   const T *tx, *tz;
   long long np, psix_plane, psiz_plane;
 };
@@ -298,6 +299,268 @@ __global__ void __launch_bounds__(256) k_stress_t(AdjArgs<T> A, Slot<T> x0, Slot
   }
 }
 
+
+// ---- S^T for TTI media --------------------------------------------------
+// The TTI stress law couples neighbouring cells (custom_solver/Model.jl:59-108
+// on the staggered grid):
+//   dsxx = C11 exx + C13 ezz + C15 ebxz,   dszz = C13 exx + C33 ezz + C35 ebxz,
+//   dsxz = C55h exz + C15h ebxx + C35h ebzz,
+// ebxz(i,j) the mean of exz over (i,j),(i-1,j),(i,j-1),(i-1,j-1), ebxx and
+// ebzz the means of exx, ezz over (i,j),(i+1,j),(i,j+1),(i+1,j+1), C15h,
+// C35h, C55h the means of the stiffness over the latter four cells, and on
+// the free surface (row L) ezz = -(C13 exx + C35 ebxz) / C33.  Effective
+// rates outside the update region U are zero.  The transpose runs in four
+// kernels: the forward rates (k_tti_fwd_rates, k_tti_fwd_surface), the
+// effective-rate adjoints gathered from the stress adjoints
+// (k_tti_ebar_t), the surface relation transposed (k_tti_surface_t) and the
+// per-cell rest — memory variables, tau, CPML psi (k_tti_stress_t).  Every
+// cell gathers its own terms: no atomics.
+template <typename T>
+__device__ __forceinline__ bool in_u(int i, int j, int nx, int nz) {
+  return i >= L && i < nx - L && j >= L && j < nz - L;
+}
+
+// Forward effective rates e (3 planes) and rt + S (3 planes: the CPML'd
+// strain rates plus the memory-variable sums, de/dtau) of step it, from the
+// new velocities (x1) and the CPML memory and memory variables before the
+// step (x0).  fe is zero outside U.
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_tti_fwd_rates(AdjArgs<T> A, Slot<T> x0, Slot<T> x1, T *fe) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
+  if (i >= A.nx - L || j >= A.nz - L) return;
+  const int nx = A.nx;
+  const long long c = (long long)j * nx + i, np = A.np;
+  T r[4];
+  r[0] = tap_m(x1.vx(), c, 1, A.Dx);
+  r[1] = tap_m(x1.vz(), c, nx, A.Dz);
+  r[2] = tap_p(x1.vx(), c, nx, A.Dz);
+  r[3] = tap_p(x1.vz(), c, 1, A.Dx);
+  const int xs = strip_x(i, nx, A.Lx, A.Rx), zs = strip_z(j, A.nz, A.Tz, A.Bz);
+  T pn;
+  if (xs >= 0) {
+    const long long o = (long long)j * A.wx + xs;
+    r[0] = cpml_fwd(r[0], x0.psix()[PX_VX * A.psix_plane + o], A.tx[T_A * nx + i], A.tx[T_B * nx + i],
+                    A.tx[T_IK * nx + i], &pn);
+    r[3] = cpml_fwd(r[3], x0.psix()[PX_VZ * A.psix_plane + o], A.tx[T_AH * nx + i], A.tx[T_BH * nx + i],
+                    A.tx[T_IKH * nx + i], &pn);
+  }
+  if (zs >= 0) {
+    const int nz = A.nz;
+    const long long o = (long long)zs * nx + i;
+    r[1] = cpml_fwd(r[1], x0.psiz()[PZ_VZ * A.psiz_plane + o], A.tz[T_A * nz + j], A.tz[T_B * nz + j],
+                    A.tz[T_IK * nz + j], &pn);
+    r[2] = cpml_fwd(r[2], x0.psiz()[PZ_VX * A.psiz_plane + o], A.tz[T_AH * nz + j], A.tz[T_BH * nz + j],
+                    A.tz[T_IKH * nz + j], &pn);
+  }
+  const T rt[3] = {r[0], r[1], r[2] + r[3]};
+  T S[3] = {0, 0, 0};
+#pragma unroll
+  for (int n = 0; n < N; ++n)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S[k] += x0.m()[(k * N + n) * np + c];
+  const T tau = N > 0 ? A.tau[c] : T(0);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    fe[k * np + c] = N > 0 ? (T(1) + tau) * rt[k] + tau * S[k] : rt[k];
+    fe[(3 + k) * np + c] = rt[k] + S[k];
+  }
+}
+
+// The free-surface relation of the forward step on row L:
+// ezz = -(C13 exx + C35 ebxz) / C33 (row L - 1 lies outside U: zero there).
+template <typename T>
+__global__ void k_tti_fwd_surface(AdjArgs<T> A, T *fe) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  if (i >= A.nx - L) return;
+  const int nx = A.nx;
+  const long long np = A.np, c = (long long)L * nx + i;
+  const T *exx = fe, *exz = fe + 2 * np;
+  const T eb = T(0.25) * (exz[c] + exz[c - 1] + exz[c - nx] + exz[c - nx - 1]);
+  fe[np + c] = -(A.c13[c] * exx[c] + A.c35[c] * eb) / A.c33[c];
+}
+
+// Adjoints of the effective rates (3 planes eb) gathered from the stress
+// adjoints of the cells whose update reads them, and the direct stiffness
+// gradient terms: C11, C13, C33, C15 and C35 at the cell, and the
+// per-cell products q (C55h), q15 (C15h), q35 (C35h) that k_gather and
+// k_tti_gather spread over the four cells of each half-node mean.  On the
+// free surface the stress szz is reset after the update, so its adjoint
+// there is zero.
+template <typename T>
+__global__ void __launch_bounds__(256) k_tti_ebar_t(AdjArgs<T> A, Slot<T> ab, const T *fe, T *eb, T *q,
+                                                     T *q15, T *q35, double *g11, double *g13, double *g15,
+                                                     double *g33, double *g35) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
+  const int nx = A.nx, nz = A.nz;
+  if (i >= nx - L || j >= nz - L) return;
+  const long long c = (long long)j * nx + i, np = A.np;
+  const T *sbx = ab.sxx(), *sbz = ab.szz(), *sbq = ab.sxz();
+  const T *exx = fe, *ezz = fe + np, *exz = fe + 2 * np;
+  const T dt = A.dt;
+  auto bzz = [&](int ii, int jj) -> T {  // szz adjoint of a cell of U (zero on the surface)
+    return (A.fs && jj == L) ? T(0) : sbz[(long long)jj * nx + ii];
+  };
+  auto mean4p = [&](const T *u, long long cc) { return T(0.25) * (u[cc] + u[cc + 1] + u[cc + nx] + u[cc + nx + 1]); };
+  const T bxx = sbx[c], bzc = bzz(i, j), bxz = sbq[c];
+  const T C11 = A.c11[c], C13 = A.c13[c], C33 = A.c33[c], C15 = A.c15[c], C35 = A.c35[c];
+  const T C55h = mean4p(A.c55, c);
+  // exz feeds sxx, szz of the cells (i,j), (i+1,j), (i,j+1), (i+1,j+1)
+  T sq = 0;
+#pragma unroll
+  for (int dj = 0; dj <= 1; ++dj)
+#pragma unroll
+    for (int di = 0; di <= 1; ++di) {
+      const int ii = i + di, jj = j + dj;
+      if (in_u<T>(ii, jj, nx, nz)) {
+        const long long cc = (long long)jj * nx + ii;
+        sq += A.c15[cc] * sbx[cc] + A.c35[cc] * bzz(ii, jj);
+      }
+    }
+  // exx, ezz feed sxz of the cells (i,j), (i-1,j), (i,j-1), (i-1,j-1)
+  T sx = 0, sz = 0;
+#pragma unroll
+  for (int dj = 0; dj <= 1; ++dj)
+#pragma unroll
+    for (int di = 0; di <= 1; ++di) {
+      const int ii = i - di, jj = j - dj;
+      if (in_u<T>(ii, jj, nx, nz)) {
+        const long long cc = (long long)jj * nx + ii;
+        sx += mean4p(A.c15, cc) * sbq[cc];
+        sz += mean4p(A.c35, cc) * sbq[cc];
+      }
+    }
+  eb[c] = dt * (C11 * bxx + C13 * bzc + T(0.25) * sx);
+  eb[np + c] = dt * (C13 * bxx + C33 * bzc + T(0.25) * sz);
+  eb[2 * np + c] = dt * (C55h * bxz + T(0.25) * sq);
+  // forward rates at the cell and the neighbour means its update used
+  const T ex = exx[c], ez = ezz[c], eq = exz[c];
+  const T ebxz = T(0.25) * (exz[c] + exz[c - 1] + exz[c - nx] + exz[c - nx - 1]);
+  const T ebxx = mean4p(exx, c), ebzz = mean4p(ezz, c);
+  g11[c] += (double)dt * bxx * ex;
+  g13[c] += (double)dt * ((double)bxx * ez + (double)bzc * ex);
+  g33[c] += (double)dt * bzc * ez;
+  g15[c] += (double)dt * bxx * ebxz;
+  g35[c] += (double)dt * bzc * ebxz;
+  q[c] = dt * bxz * eq;
+  q15[c] = dt * bxz * ebxx;
+  q35[c] = dt * bxz * ebzz;
+}
+
+// The surface relation transposed (row L): the adjoint of the surface ezz
+// (as k_tti_ebar_t gathered it) moves to exx of the cell and to exz of the
+// cell and its left neighbour, and adds its stiffness terms; the surface
+// ezz adjoint itself is read as zero afterwards (k_tti_stress_t).
+template <typename T>
+__global__ void k_tti_surface_t(AdjArgs<T> A, const T *fe, T *eb, double *g13, double *g33, double *g35) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int nx = A.nx;
+  if (i >= nx - L) return;
+  const long long np = A.np, c = (long long)L * nx + i;
+  const T *exx = fe, *ezz = fe + np, *exz = fe + 2 * np;
+  const T zb = eb[np + c];
+  const T C33 = A.c33[c];
+  eb[c] += -A.c13[c] / C33 * zb;
+  T xz = -T(0.25) * A.c35[c] / C33 * zb;
+  if (i + 1 < nx - L) xz -= T(0.25) * A.c35[c + 1] / A.c33[c + 1] * eb[np + c + 1];
+  eb[2 * np + c] += xz;
+  const T ebs = T(0.25) * (exz[c] + exz[c - 1] + exz[c - nx] + exz[c - nx - 1]);
+  g13[c] += -(double)zb * exx[c] / C33;
+  g35[c] += -(double)zb * ebs / C33;
+  g33[c] += -(double)zb * ezz[c] / C33;
+}
+
+// Memory variables, the tau gradient and the CPML psi transposes of a TTI
+// cell, from the effective-rate adjoints: rbar (4 planes) as k_stress_t
+// leaves it.
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_tti_stress_t(AdjArgs<T> A, Slot<T> ab, const T *fe, const T *eb,
+                                                       T *rbar, double *gtau) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
+  const int nx = A.nx;
+  if (i >= nx - L || j >= A.nz - L) return;
+  const long long c = (long long)j * nx + i, np = A.np;
+  const bool surf = A.fs && j == L;
+  T e_b[3] = {eb[c], surf ? T(0) : eb[np + c], eb[2 * np + c]};
+  if (surf) ab.szz()[c] = T(0);
+  const T tau = N > 0 ? A.tau[c] : T(0);
+  if (N > 0) {
+    double gt = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) gt += (double)e_b[k] * fe[(3 + k) * np + c];
+    gtau[c] += gt;
+  }
+  T rtb[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) rtb[k] = (N > 0 ? (T(1) + tau) : T(1)) * e_b[k];
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const bool dead = surf && k == 1;  // Mzz' = 0 on the surface
+      T *mp = ab.m() + (k * N + n) * np + c;
+      const T mb = dead ? T(0) : *mp;
+      rtb[k] += A.dt * A.a1[n] * mb;
+      *mp = dead ? T(0) : tau * e_b[k] + mb * (T(1) + A.dt * A.a2[n]);
+    }
+  }
+  T ik[4] = {1, 1, 1, 1}, ca[4] = {0, 0, 0, 0}, cb[4] = {0, 0, 0, 0};
+  T *pb[4] = {nullptr, nullptr, nullptr, nullptr};
+  const int xs = strip_x(i, nx, A.Lx, A.Rx), zs = strip_z(j, A.nz, A.Tz, A.Bz);
+  if (xs >= 0) {
+    const long long o = (long long)j * A.wx + xs;
+    ik[0] = A.tx[T_IK * nx + i]; ca[0] = A.tx[T_A * nx + i]; cb[0] = A.tx[T_B * nx + i];
+    ik[3] = A.tx[T_IKH * nx + i]; ca[3] = A.tx[T_AH * nx + i]; cb[3] = A.tx[T_BH * nx + i];
+    pb[0] = ab.psix() + PX_VX * A.psix_plane + o;
+    pb[3] = ab.psix() + PX_VZ * A.psix_plane + o;
+  }
+  if (zs >= 0) {
+    const int nz = A.nz;
+    const long long o = (long long)zs * nx + i;
+    ik[1] = A.tz[T_IK * nz + j]; ca[1] = A.tz[T_A * nz + j]; cb[1] = A.tz[T_B * nz + j];
+    ik[2] = A.tz[T_IKH * nz + j]; ca[2] = A.tz[T_AH * nz + j]; cb[2] = A.tz[T_BH * nz + j];
+    pb[1] = ab.psiz() + PZ_VZ * A.psiz_plane + o;
+    pb[2] = ab.psiz() + PZ_VX * A.psiz_plane + o;
+  }
+  T rb[4] = {rtb[0], rtb[1], rtb[2], rtb[2]};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (pb[k]) {
+      const T P = *pb[k] + rb[k];
+      *pb[k] = cb[k] * P;
+      rb[k] = rb[k] * ik[k] + ca[k] * P;
+    }
+    rbar[k * np + c] = rb[k];
+  }
+}
+
+// C15 and C35 gather the half-node products of the four means they enter
+// (as k_gather does for C55)
+template <typename T>
+__global__ void k_tti_gather(const T *q15, const T *q35, double *g15, double *g35, int nx, int nz) {
+  pdl_wait();  // launched while the previous kernel drains
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= nx || j >= nz) return;
+  const long long c = (long long)j * nx + i;
+  double t15 = 0, t35 = 0;
+  for (int dj = 0; dj <= 1; ++dj)
+    for (int di = 0; di <= 1; ++di) {
+      const int ii = i - di, jj = j - dj;
+      if (ii >= 0 && jj >= 0) {
+        t15 += q15[(long long)jj * nx + ii];
+        t35 += q35[(long long)jj * nx + ii];
+      }
+    }
+  g15[c] += 0.25 * t15;
+  g35[c] += 0.25 * t35;
+}
 
 // v += -D^T rbar over the update region (its taps reach at most L cells,
 // so they stay inside the planes; rbar is zero outside the region)
@@ -592,6 +855,64 @@ __global__ void k_thomsen_grad(long long np, const double *g, const double *vp, 
   out[1 * np + c] = g13 * A * C33 / sq;  // dJ/ddelta
 }
 
+// Forward-mode derivative pairs (value, d/dp) for the TTI chain rule.
+struct Dual {
+  double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator*(double s, Dual a) { return {s * a.v, s * a.d}; }
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+  const double r = sqrt(fmax(a.v, 1e-300));
+  return {r, a.d / (2.0 * r)};
+}
+
+// The TTI stiffness of one cell from (vp, vs, rho, epsilon, delta, theta):
+// Thomsen's VTI law (Models.jl:27-52, custom_solver/Model.jl:12-16) tilted
+// by the 2D Bond rotation (the map of vi_medium_from_velocity), carried on
+// derivative pairs.  out = (C11, C13, C15, C33, C35, C55).
+__device__ __forceinline__ void tti_stiffness(Dual p, Dual s, Dual r, Dual e, Dual d, Dual th, Dual (&out)[6]) {
+  const Dual C33 = r * p * p, C55 = r * s * s;
+  const Dual C11 = C33 * Dual{1.0 + 2.0 * e.v, 2.0 * e.d};
+  const Dual C13 = dsqrt((C33 - C55) * (C33 * Dual{1.0 + 2.0 * d.v, 2.0 * d.d} - C55)) - C55;
+  const Dual co{cos(th.v), -sin(th.v) * th.d}, si{sin(th.v), cos(th.v) * th.d};
+  const Dual c2 = co * co, s2 = si * si, cs = co * si, A = C13 + 2.0 * C55, dcs = c2 - s2;
+  out[0] = c2 * c2 * C11 + 2.0 * (c2 * s2 * A) + s2 * s2 * C33;
+  out[1] = c2 * s2 * (C11 + C33 - 4.0 * C55) + (c2 * c2 + s2 * s2) * C13;
+  out[2] = -1.0 * (cs * (c2 * C11 - s2 * C33 - dcs * A));
+  out[3] = s2 * s2 * C11 + 2.0 * (c2 * s2 * A) + c2 * c2 * C33;
+  out[4] = -1.0 * (cs * (s2 * C11 - c2 * C33 + dcs * A));
+  out[5] = c2 * s2 * (C11 + C33 - 2.0 * C13) + dcs * dcs * C55;
+}
+
+// dJ/d(vp, vs, rho, 1/Q, epsilon, delta, theta) of a TTI medium from the
+// stiffness gradient g (vi_gradient's eight planes): the chain rule through
+// tti_stiffness, one derivative direction per parameter.
+__global__ void k_tti_param_grad(long long np, const double *g, const double *vp, const double *vs,
+                                 const double *rho, const double *eps, const double *delta,
+                                 const double *theta, double tau_scale, double *out) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= np) return;
+  const double gk[6] = {g[1 * np + c], g[2 * np + c], g[3 * np + c], g[4 * np + c], g[5 * np + c], g[6 * np + c]};
+  const double val[6] = {vp[c], vs[c], rho[c], eps ? eps[c] : 0.0, delta ? delta[c] : 0.0, theta ? theta[c] : 0.0};
+  const int slot[6] = {0, 1, 2, 4, 5, 6};  // output plane of each parameter (3 is 1/Q)
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    Dual x[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) x[k] = {val[k], k == q ? 1.0 : 0.0};
+    Dual C[6];
+    tti_stiffness(x[0], x[1], x[2], x[3], x[4], x[5], C);
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += gk[k] * C[k].d;
+    if (q == 2) s += g[c];  // rho also enters the buoyancy directly
+    out[slot[q] * np + c] = s;
+  }
+  out[3 * np + c] = g[7 * np + c] * tau_scale;  // dJ/d(1/Q)
+}
+
 __global__ void k_fold_iso(long long np, double *g) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= np) return;
@@ -609,7 +930,9 @@ template <typename T>
 static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, int nt, const T *obs,
                          int K, int accumulate, double *grad, double *misfit, cudaStream_t st) {
   const vi_config &c = p->cfg;
-  if (c.medium == VI_MEDIUM_TTI) return set_error(VI_ERR_ARG, "gradient: TTI media are not supported");
+  const bool tti = c.medium == VI_MEDIUM_TTI;
+  if (c.free_surface == kFsAfda)
+    return set_error(VI_ERR_ARG, "gradient: the adjoint covers the stress-imaging free surface, not H-AFDA");
   int rc = check_medium(p, m);
   if (rc) return rc;
   if (!shot || shot->nrec <= 0 || !obs) return set_error(VI_ERR_ARG, "gradient: needs receivers and observed traces");
@@ -622,10 +945,12 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   const long long np = (long long)c.nx * c.nz;
   const int N = c.nsls;
   const long long slot = Slot<T>::size(np, p->psix_plane, p->psiz_plane, N);
-  // workspace: checkpoints | segment (K + 1 slots) | adjoint slot | scratch (4 rbar/dbar, q, 2 h, 6 plain) | traces
+  // workspace: checkpoints | segment (K + 1 slots) | adjoint slot | scratch (4 rbar/dbar, q, 2 h, 6 plain
+  // (TTI: also the forward effective rates of the adjoint sweep), TTI: 3 effective-rate adjoints, q15, q35) |
+  // traces
   const int nrec = shot->nrec;
   const long long ntr = 2LL * nrec * nt;
-  const long long scratch = 4 * np + np + 2 * np + 6 * np;
+  const long long scratch = 4 * np + np + 2 * np + 6 * np + (tti ? 5 * np : 0);
   const size_t need = sizeof(T) * ((size_t)(nck + K + 2) * slot + scratch + ntr) + 64;
   size_t have = p->fwd_bytes;
   if ((rc = ensure_buffer(p, &p->fwd, &have, need))) return rc;
@@ -637,7 +962,9 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   T *q = rbar + 4 * np;
   T *h = q + np;
   T *pscr = h + 2 * np;   // plain-path scratch (6 planes)
-  T *tr = pscr + 6 * np;
+  T *teb = pscr + 6 * np;  // TTI: effective-rate adjoints (3 planes), q15, q35
+  T *tq15 = teb + 3 * np, *tq35 = tq15 + np;
+  T *tr = pscr + 6 * np + (tti ? 5 * np : 0);
   auto mk = [&](T *b) { return Slot<T>{b, np, p->psix_plane, p->psiz_plane, N}; };
   if ((rc = stage_shot<T>(p, shot, st))) return rc;
   // plain forward step on a slot, in place (bind() points it at the slot)
@@ -674,7 +1001,10 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   using SG = SplitGeom<T>;
   StepArgs<T> probe = a;
   bind(probe, mk(seg));
-  const bool use_split = split_eligible<T>(p, probe);
+  // TTI sweeps run the plain path (the TTI split pass has no out-of-place
+  // form); the 4-cell transposed derivatives only need aligned planes
+  const bool split_ok = split_eligible<T>(p, probe);
+  const bool use_split = split_ok && !tti;
   using SS = SplitStressGeom<T>;
   FusedExtras<T> fx{}, fxs{};
   SplitMaps ms{};
@@ -776,21 +1106,23 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   }
   A.rho = (const T *)m->rho; A.c11 = (const T *)m->c11; A.c13 = (const T *)m->c13;
   A.c33 = (const T *)m->c33; A.c55 = (const T *)m->c55; A.tau = (const T *)m->tau;
+  A.c15 = (const T *)m->c15; A.c35 = (const T *)m->c35;
   A.tx = (const T *)p->tabx; A.tz = (const T *)p->tabz;
   A.np = np; A.psix_plane = p->psix_plane; A.psiz_plane = p->psiz_plane;
   Slot<T> ab = mk(adj);
   if ((rc = cuda_check(cudaMemsetAsync(adj, 0, sbytes, st), "zero adjoint"))) return rc;
   if ((rc = cuda_check(cudaMemsetAsync(rbar, 0, 7 * np * sizeof(T), st), "zero scratch"))) return rc;
+  if (tti && (rc = cuda_check(cudaMemsetAsync(teb, 0, 5 * np * sizeof(T), st), "zero TTI scratch"))) return rc;
   if (!accumulate)
     if ((rc = cuda_check(cudaMemsetAsync(grad, 0, 8 * np * sizeof(double), st), "zero gradient"))) return rc;
   double *gr = grad, *g11 = grad + np, *g13 = grad + 2 * np, *g33 = grad + 4 * np;
-  double *g55 = grad + 6 * np, *gt = grad + 7 * np;
+  double *g55 = grad + 6 * np, *gt = grad + 7 * np, *g15 = grad + 3 * np, *g35 = grad + 5 * np;
   const dim3 blk(32, 8);
   const dim3 gU((c.nx - 2 * L + 31) / 32, (c.nz - 2 * L + 7) / 8);
   const dim3 gA((c.nx + 31) / 32, (c.nz + 7) / 8);
   // 4-cell forms of the transposed derivatives where the planes allow
   // 128-bit access (the same condition as the split pair)
-  const bool vec4 = use_split;
+  const bool vec4 = split_ok;
   const dim3 gU4(((c.nx - 2 * L) / 4 + 31) / 32, (c.nz - 2 * L + 7) / 8);
   const dim3 gA4((c.nx / 4 + 31) / 32, (c.nz + 7) / 8);
   int lrc = VI_OK;  // first launch error of the adjoint sweep
@@ -822,7 +1154,28 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
       // every kernel of the step overlaps its predecessor's tail and waits
       // for it at entry (programmatic dependent launch)
       if (c.free_surface) lc(k_mirror_t<T>, dim3((c.nx + 127) / 128), dim3(128), ab.szz(), ab.sxz(), c.nx);
-      switch (N) {
+      if (tti) {
+        const dim3 gS((c.nx - 2 * L + 127) / 128);
+        switch (N) {
+          case 0: lc(k_tti_fwd_rates<T, 0>, gU, blk, A, x0, x1, pscr); break;
+          case 1: lc(k_tti_fwd_rates<T, 1>, gU, blk, A, x0, x1, pscr); break;
+          case 2: lc(k_tti_fwd_rates<T, 2>, gU, blk, A, x0, x1, pscr); break;
+          case 3: lc(k_tti_fwd_rates<T, 3>, gU, blk, A, x0, x1, pscr); break;
+          case 4: lc(k_tti_fwd_rates<T, 4>, gU, blk, A, x0, x1, pscr); break;
+          default: lc(k_tti_fwd_rates<T, 5>, gU, blk, A, x0, x1, pscr); break;
+        }
+        if (c.free_surface) lc(k_tti_fwd_surface<T>, gS, dim3(128), A, pscr);
+        lc(k_tti_ebar_t<T>, gU, blk, A, ab, (const T *)pscr, teb, q, tq15, tq35, g11, g13, g15, g33, g35);
+        if (c.free_surface) lc(k_tti_surface_t<T>, gS, dim3(128), A, (const T *)pscr, teb, g13, g33, g35);
+        switch (N) {
+          case 0: lc(k_tti_stress_t<T, 0>, gU, blk, A, ab, (const T *)pscr, (const T *)teb, rbar, gt); break;
+          case 1: lc(k_tti_stress_t<T, 1>, gU, blk, A, ab, (const T *)pscr, (const T *)teb, rbar, gt); break;
+          case 2: lc(k_tti_stress_t<T, 2>, gU, blk, A, ab, (const T *)pscr, (const T *)teb, rbar, gt); break;
+          case 3: lc(k_tti_stress_t<T, 3>, gU, blk, A, ab, (const T *)pscr, (const T *)teb, rbar, gt); break;
+          case 4: lc(k_tti_stress_t<T, 4>, gU, blk, A, ab, (const T *)pscr, (const T *)teb, rbar, gt); break;
+          default: lc(k_tti_stress_t<T, 5>, gU, blk, A, ab, (const T *)pscr, (const T *)teb, rbar, gt); break;
+        }
+      } else switch (N) {
         case 0: lc(k_stress_t<T, 0>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
         case 1: lc(k_stress_t<T, 1>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
         case 2: lc(k_stress_t<T, 2>, gU, blk, A, x0, x1, ab, rbar, q, g11, g13, g33, gt); break;
@@ -840,6 +1193,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
         lc(k_force_rho_t<T>, dim3((shot->nsrc + 127) / 128), dim3(128), A, ab, (const int4 *)p->dsrc,
            (const T *)p->damp, shot->nsrc, (const T *)shot->wavelet_dev, shot->wavelet_nt, it, h);
       lc(k_gather<T>, gA, blk, (const T *)h, gr, (const T *)q, g55, c.nx, c.nz);
+      if (tti) lc(k_tti_gather<T>, gA, blk, (const T *)tq15, (const T *)tq35, g15, g35, c.nx, c.nz);
       if (vec4)
         lc(k_div_t4<T>, gA4, blk, A, ab, (const T *)rbar);
       else
@@ -881,6 +1235,16 @@ extern "C" int vi_gradient_velocity(int32_t medium, int64_t np, const double *gr
   k_velocity_grad<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       medium, np, grad8, vp, vs, rho, eps, delta, tau_scale, out4);
   return cuda_check(cudaGetLastError(), "gradient_velocity launch");
+}
+
+extern "C" int vi_gradient_tti(int64_t np, const double *grad8, const double *vp, const double *vs,
+                               const double *rho, const double *eps, const double *delta, const double *theta,
+                               double tau_scale, double *out7, void *stream) {
+  if (!grad8 || !vp || !vs || !rho || !out7 || np <= 0)
+    return set_error(VI_ERR_ARG, "gradient_tti: NULL argument");
+  k_tti_param_grad<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(np, grad8, vp, vs, rho, eps,
+                                                                                   delta, theta, tau_scale, out7);
+  return cuda_check(cudaGetLastError(), "gradient_tti launch");
 }
 
 extern "C" int vi_gradient_thomsen(int64_t np, const double *grad8, const double *vp, const double *vs,

@@ -52,6 +52,7 @@ struct vi_batch {
   std::vector<int> order;
   std::vector<int> prefix;
   int max_nt = 0;
+  bool afda = false;  // some shot has the H-AFDA free surface
 };
 
 namespace vb {
@@ -133,6 +134,18 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
     if (split) {
       if (!split_eligible<T>(p, a))
         return set_error(VI_ERR_ARG, "batch: the split step needs 16-byte aligned planes");
+      if (b->precision == VI_F32C) {
+        // compensated stress accumulation, as the shot's own split step
+        if (!p->slo) {
+          size_t have = 0;
+          if ((rc = ensure_buffer(p, &p->slo, &have, 3 * np * sizeof(uint16_t)))) return rc;
+          if ((rc = cuda_check(cudaMemsetAsync(p->slo, 0, 3 * np * sizeof(uint16_t), st), "zero stress residues")))
+            return rc;
+          p->slo_valid = true;
+        }
+        a.slo = (uint16_t *)p->slo;
+        a.slo_plane = (long long)np;
+      }
       for (int par = 0; par < 2; ++par) {
         // sigma and v in place; TTI: M and psi from parity par to the other
         StepArgs<T> s = a;
@@ -257,8 +270,9 @@ static int launch_steps(vi_batch *b, const BatchDev<T> &bd, int form, int it0, i
     if (form == kFormSplit) {
       // each launch overlaps the tail of the previous one and waits for it
       // at entry (programmatic dependent launch), as the one-shot pair does
-      rc = launch_split_vel_batch<T>(b->kind, bd, it, nitems, st, it > it0);
-      if (!rc) rc = launch_split_stress_batch<T>(b->kind, b->nsls, bd, it, nitems, st, true);
+      rc = launch_split_vel_batch<T>(b->kind, b->afda, bd, it, nitems, st, it > it0);
+      if (!rc)
+        rc = launch_split_stress_batch<T>(b->kind, b->nsls, b->precision == VI_F32C, bd, it, nitems, st, true);
     } else {
       rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, it, nitems, b->nsm, form == kFormTwoStage, st);
     }
@@ -342,9 +356,10 @@ static int tune(vi_batch *b, cudaStream_t st) {
   set_order(b);
   float best = 1e30f;
   int choice = kFormTwoStage;
-  // double precision has one fused form (two stages do not fit)
+  // double precision has one fused form (two stages do not fit); compensated
+  // FP32 and the H-AFDA surface run on the split pair only
   const int forms[4] = {kFormPerShot, kFormSplit, kFormTwoStage, kFormOneStage};
-  const int nforms = sizeof(T) == 4 ? 4 : 3;
+  const int nforms = (b->precision == VI_F32C || b->afda) ? 2 : sizeof(T) == 4 ? 4 : 3;
   for (int f = 0; f < nforms; ++f) {
     const int form = forms[f];
     float ms = 0;
@@ -376,7 +391,8 @@ static int tune(vi_batch *b, cudaStream_t st) {
 // Sets kernel attributes (outside a capture) for a form.
 template <typename T>
 static int set_up_form(vi_batch *b, const BatchDev<T> &bd, int form, cudaStream_t st) {
-  if (form == kFormSplit) return launch_split_stress_batch<T>(b->kind, b->nsls, bd, 0, 0, st, false);
+  if (form == kFormSplit)
+    return launch_split_stress_batch<T>(b->kind, b->nsls, b->precision == VI_F32C, bd, 0, 0, st, false);
   return launch_fused_tma_batch<T>(b->kind, b->nsls, bd, 0, 0, b->nsm, form == kFormTwoStage, st);
 }
 
@@ -457,6 +473,15 @@ static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
                            "copy back memory variables")))
         return rc;
   }
+  // the fused forms do not fold the finite check into their stress pass:
+  // check every shot's stresses once at the end of the run
+  if (form != kFormSplit)
+    for (int i = 0; i < b->n; ++i) {
+      const vi_fields &f = b->fields[i];
+      const vi_plan *p = b->plans[i];
+      if ((rc = launch_finite_check<T>(f.sxx, f.szz, f.sxz, (long long)p->cfg.nx * p->cfg.nz, b->err, b->nsm, st)))
+        return rc;
+    }
   return cuda_check(cudaGetLastError(), "batch run");
 }
 
@@ -491,6 +516,7 @@ extern "C" int vi_batch_create(const vi_config *cfgs, int32_t nshots, vi_batch *
       vi_batch_destroy(b);
       return rc;
     }
+    b->afda |= cfgs[i].free_surface == kFsAfda;
   }
   b->med.assign(nshots, vi_medium{});
   b->fields.assign(nshots, vi_fields{});
@@ -558,9 +584,19 @@ extern "C" int vi_batch_status(vi_batch *b, void *stream, int32_t *kernel_form) 
   int flag = 0;
   rc = cuda_check(cudaMemcpy(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
   if (rc) return rc;
+  // the per-shot form reports through each shot's plan
+  for (int i = 0; i < b->n; ++i) {
+    int pf = 0;
+    if ((rc = cuda_check(cudaMemcpy(&pf, b->plans[i]->errflag, sizeof(int), cudaMemcpyDeviceToHost),
+                         "read plan error word")))
+      return rc;
+    if (pf) cudaMemset(b->plans[i]->errflag, 0, sizeof(int));
+    flag |= pf;
+  }
   if (flag) {
     cudaMemset(b->err, 0, sizeof(int));
-    return set_error(VI_ERR_TIMEOUT, "batch: a bounded device wait gave up");
+    if (flag & kErrTimeout) return set_error(VI_ERR_TIMEOUT, "batch: a bounded device wait gave up");
+    return set_error(VI_ERR_NONFINITE, "batch: a stress value came out NaN or infinite");
   }
   return VI_OK;
 }

@@ -1,4 +1,5 @@
 // capi.cu — C ABI (include/visco_b200.h): plan, time stepping, forward solve.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -82,6 +83,68 @@ static void cpml_tables(const vi_config &c, int axis, int half, double *ik, doub
   }
 }
 
+// Weights of the first derivative at x0 from the samples at x[0..n-1]
+// (n <= 8): sum_k w_k (x_k - x0)^l / l! = [l == 1] for l < n — the
+// Vandermonde system of Stencil.jl:_stencil (lines 9-14), solved by
+// Gaussian elimination with partial pivoting.
+static void fd_weights(const double *x, int n, double x0, double *w) {
+  double A[8][9];
+  for (int l = 0; l < n; ++l) {
+    double fact = 1;
+    for (int q = 2; q <= l; ++q) fact *= q;
+    for (int k = 0; k < n; ++k) A[l][k] = std::pow(x[k] - x0, l) / fact;
+    A[l][n] = l == 1 ? 1.0 : 0.0;
+  }
+  for (int c = 0; c < n; ++c) {
+    int p = c;
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(A[r][c]) > std::fabs(A[p][c])) p = r;
+    for (int k = 0; k <= n; ++k) std::swap(A[c][k], A[p][k]);
+    for (int r = 0; r < n; ++r)
+      if (r != c && A[r][c] != 0) {
+        const double f = A[r][c] / A[c][c];
+        for (int k = c; k <= n; ++k) A[r][k] -= f * A[c][k];
+      }
+  }
+  for (int k = 0; k < n; ++k) w[k] = A[k][n] / A[k][k];
+}
+
+// H-AFDA free surface (Kristek, Moczo & Archuleta 2002, the reference's
+// FreeSurfaceStencil, Stencil.jl:52-105, and kernels,
+// free-surface-kernels.jl:16-213): the surface z = 0 is the row of sxx,
+// szz and vx; szz(0) = sxz(0) = 0 there and nothing lives above it.  A z
+// derivative whose 8th-order staggered stencil would reach above the
+// surface takes a one-sided approximation from kAfdaN samples at or below
+// it (plus the zero boundary value of sxz or szz at z = 0) — unit-spacing
+// weights w[op][q][m] in the layout of StepArgs::af.  The reference sizes
+// these approximations like the interior stencil (8 samples); with 8 the
+// semi-discrete operator has growing modes, with 5 it has none.
+static void afda_unit_weights(double w[4][4][kAfdaN]) {
+  double x[kAfdaN + 1], t[kAfdaN + 1];
+  std::memset(w, 0, sizeof(double) * 4 * 4 * kAfdaN);
+  for (int q = 0; q < 4; ++q) {  // d(sxz)/dz at z = q from sxz(0) = 0 and sxz at m + 1/2
+    x[0] = 0;
+    for (int m = 0; m < kAfdaN; ++m) x[m + 1] = m + 0.5;
+    fd_weights(x, kAfdaN + 1, q, t);
+    for (int m = 0; m < kAfdaN; ++m) w[0][q][m] = t[m + 1];
+  }
+  for (int q = 0; q < 3; ++q) {  // d(szz)/dz at z = q + 1/2 from szz(0) = 0 and szz at 1 + m
+    for (int m = 0; m <= kAfdaN; ++m) x[m] = m;
+    fd_weights(x, kAfdaN + 1, q + 0.5, t);
+    for (int m = 0; m < kAfdaN; ++m) w[1][q][m] = t[m + 1];
+  }
+  for (int q = 1; q < 4; ++q) {  // d(vz)/dz at z = q from vz at m + 1/2
+    for (int m = 0; m < kAfdaN; ++m) x[m] = m + 0.5;
+    fd_weights(x, kAfdaN, q, t);
+    for (int m = 0; m < kAfdaN; ++m) w[2][q][m] = t[m];
+  }
+  for (int q = 0; q < 3; ++q) {  // d(vx)/dz at z = q + 1/2 from vx at m
+    for (int m = 0; m < kAfdaN; ++m) x[m] = m;
+    fd_weights(x, kAfdaN, q + 0.5, t);
+    for (int m = 0; m < kAfdaN; ++m) w[3][q][m] = t[m];
+  }
+}
+
 static int validate(const vi_config *c) {
   if (!c) return set_error(VI_ERR_ARG, "config is NULL");
   if (c->nx < 2 * L + 2 || c->nz < 2 * L + 2)
@@ -92,7 +155,7 @@ static int validate(const vi_config *c) {
     return set_error(VI_ERR_ARG, "dx, dz and dt must be positive");
   if (c->medium < VI_MEDIUM_ISO || c->medium > VI_MEDIUM_TTI)
     return set_error(VI_ERR_ARG, "unknown medium kind");
-  if (c->precision != VI_F32 && c->precision != VI_F64)
+  if (c->precision != VI_F32 && c->precision != VI_F64 && c->precision != VI_F32C)
     return set_error(VI_ERR_ARG, "unknown precision");
   if (c->nsls < 0 || c->nsls > VI_MAX_SLS)
     return set_error(VI_ERR_ARG, "nsls must be in 0..5");
@@ -108,6 +171,8 @@ static int validate(const vi_config *c) {
       return set_error(VI_ERR_ARG, "CPML d0 needs vmax > 0 and 0 < R < 1");
     if (c->pml_kappa_max < 1) return set_error(VI_ERR_ARG, "CPML kappa_max must be >= 1");
   }
+  if (c->free_surface < 0 || c->free_surface > kFsAfda)
+    return set_error(VI_ERR_ARG, "free_surface must be 0 (none), 1 (stress imaging) or 2 (H-AFDA)");
   if (c->free_surface && c->pml_top && c->pml_thickness > 0)
     return set_error(VI_ERR_ARG, "free surface and a top CPML are exclusive");
   if (c->pml_vmax > 0) {
@@ -156,6 +221,13 @@ StepArgs<T> make_args(const vi_plan *p, const vi_medium *m, const vi_fields *f) 
   for (int n = 0; n < c.nsls; ++n) {
     a.a1[n] = (T)(-1.0 / (c.nsls * c.tau_sls[n]));
     a.a2[n] = (T)(-1.0 / c.tau_sls[n]);
+  }
+  if (c.free_surface == kFsAfda) {
+    double w[4][4][kAfdaN];
+    afda_unit_weights(w);
+    for (int op = 0; op < 4; ++op)
+      for (int q = 0; q < 4; ++q)
+        for (int k = 0; k < kAfdaN; ++k) a.af[op][q][k] = (T)(w[op][q][k] / c.dz);
   }
   a.rho = (const T *)m->rho;
   a.c11 = (const T *)m->c11;
@@ -273,6 +345,30 @@ int stage_shot(vi_plan *p, const vi_shot *s, cudaStream_t st) {
   return VI_OK;
 }
 
+// Finite check of the stresses after a call of the step paths that do not
+// fold it into their stress pass (the split pair does): one warp vote per
+// 32 cells, the error word's non-finite bit on any NaN or infinity.
+template <typename T>
+__global__ void k_finite(const T *sxx, const T *szz, const T *sxz, long long np, int *err) {
+  bool bad = false;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < np; c += (long long)gridDim.x * blockDim.x)
+    bad |= !isfinite(sxx[c] + szz[c] + sxz[c]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, kErrNonFinite);
+}
+
+template <typename T>
+int launch_finite_check(const void *sxx, const void *szz, const void *sxz, long long np, int *err, int nsm,
+                        cudaStream_t st) {
+  if (np <= 0) return VI_OK;
+  k_finite<T><<<(unsigned)std::min<long long>(4LL * nsm, (np + 255) / 256), 256, 0, st>>>(
+      (const T *)sxx, (const T *)szz, (const T *)sxz, np, err);
+  return cuda_check(cudaGetLastError(), "finite check launch");
+}
+template int launch_finite_check<float>(const void *, const void *, const void *, long long, int *, int,
+                                        cudaStream_t);
+template int launch_finite_check<double>(const void *, const void *, const void *, long long, int *, int,
+                                         cudaStream_t);
+
 template <typename T>
 static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot *s, int it0,
                      int nsteps, int variant, cudaStream_t st) {
@@ -291,6 +387,14 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   StepArgs<T> a = make_args<T>(p, m, f);
   const int nsrc = s ? s->nsrc : 0;
   const int nrec = s ? s->nrec : 0;
+  if (p->cfg.precision == VI_F32C && (variant == 1 || variant == 7))
+    return set_error(VI_ERR_ARG, "compensated FP32 (VI_F32C) runs on the split pair only (kernel variant 0, 5 or 8)");
+  if (p->cfg.free_surface == kFsAfda) {
+    if (variant == 2 || variant == 3 || variant == 4 || variant == 6 || variant == 7)
+      return set_error(VI_ERR_ARG, "the H-AFDA free surface runs on the split pair and the plain path "
+                                   "(kernel variant 0, 1, 5 or 8)");
+    if (variant == 0 && !split_eligible<T>(p, a) && p->cfg.precision != VI_F32C) variant = 1;
+  }
   if (variant == 1) {
     if (!p->scratch) {
       // cells outside the update region are read by the neighbour averages
@@ -327,6 +431,10 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     } else {
       return set_error(VI_ERR_ARG, "the streaming step is FP32 only");
     }
+  } else if (p->cfg.precision == VI_F32C &&
+             !(variant == 5 || variant == 8 || (variant == 0 && split_eligible<T>(p, a)))) {
+    return set_error(VI_ERR_ARG, "compensated FP32 (VI_F32C) runs on the split pair only (kernel variant 0, 5 or 8 "
+                                 "with nx % 4 == 0 and 16-byte aligned planes)");
   } else if (variant == 5 || variant == 6 || variant == 8 || (variant == 0 && split_eligible<T>(p, a))) {
     // the one-tile-per-CTA pair measures faster than the pipelined pair on
     // B200 (2048 x 1024 VTI: 27.6 vs 24.4 Gpt/s), so it is the default
@@ -340,6 +448,14 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     p->last_kernel = p->last_used_tma ? (variant == 4 ? 4 : 3) : 2;
   }
   if (variant == 1) p->last_kernel = 1;
+  // paths without the folded finite check get it once at the end of the call
+  if (variant == 1 || variant == 7 || p->last_kernel == 2 || p->last_kernel == 3 || p->last_kernel == 4 ||
+      p->last_kernel == 6) {
+    if (nsteps > 0 &&
+        (rc = launch_finite_check<T>(a.sxx, a.szz, a.sxz, (long long)p->cfg.nx * p->cfg.nz, (int *)p->errflag,
+                                     p->nsm, st)))
+      return rc;
+  }
   return cuda_check(cudaGetLastError(), "step launch");
 }
 
@@ -426,7 +542,7 @@ extern "C" int vi_plan_destroy(vi_plan *p) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(p->device);
-  void *bufs[] = {p->psix, p->psiz, p->tabx, p->tabz, p->scratch, p->alt,
+  void *bufs[] = {p->psix, p->psiz, p->tabx, p->tabz, p->scratch, p->alt, p->slo,
                   p->dsrc, p->damp, p->drec, p->tile_lists, p->fwd, p->errflag};
   for (void *b : bufs)
     if (b) cudaFree(b);
@@ -443,6 +559,10 @@ extern "C" int vi_plan_reset(vi_plan *p, void *stream) {
     return rc;
   if (p->psiz && (rc = cuda_check(cudaMemsetAsync(p->psiz, 0, kPsiPlanes * (size_t)p->psiz_plane * p->esize, st), "reset psi z")))
     return rc;
+  if (p->slo && (rc = cuda_check(cudaMemsetAsync(p->slo, 0, 3 * (size_t)p->cfg.nx * p->cfg.nz * sizeof(uint16_t), st),
+                                 "reset stress residues")))
+    return rc;
+  p->slo_valid = true;
   return VI_OK;
 }
 
@@ -455,7 +575,10 @@ extern "C" int vi_plan_status(vi_plan *p, void *stream) {
   if (rc) return rc;
   if (flag) {
     cudaMemset(p->errflag, 0, sizeof(int));
-    return set_error(VI_ERR_TIMEOUT, "a bounded device wait gave up (tile staging did not complete)");
+    if (flag & kErrTimeout)
+      return set_error(VI_ERR_TIMEOUT, "a bounded device wait gave up (tile staging did not complete)");
+    return set_error(VI_ERR_NONFINITE,
+                     "a stress value came out NaN or infinite (non-finite medium or state, or an unstable run)");
   }
   return VI_OK;
 }

@@ -59,7 +59,28 @@ struct StepArgs {
   long long psix_plane, psiz_plane;
   // coefficient tables: [ik, a, b, ikh, ah, bh] x n
   const T *tx, *tz;
+  // compensated stress accumulation (FP32 split step; nullptr: off): the
+  // rounding residue of sxx, szz, sxz per cell as bfloat16 bits, 3 planes
+  // of slo_plane elements.  The stress update adds each increment to
+  // sigma + residue with an error-free two-sum and keeps the new residue.
+  uint16_t *slo;
+  long long slo_plane;
+  // H-AFDA free surface (free_surface == 2): weights / dz of the adjusted
+  // one-sided z derivatives near the surface, af[op][q][m] (kAfdaN samples):
+  // op 0 d(sxz)/dz at the vx row VI_HALF + q (samples sxz rows VI_HALF + m),
+  // op 1 d(szz)/dz at the vz row VI_HALF + q (szz rows VI_HALF + 1 + m),
+  // op 2 d(vz)/dz at the szz row VI_HALF + q (vz rows VI_HALF + m, q >= 1),
+  // op 3 d(vx)/dz at the sxz row VI_HALF + q (vx rows VI_HALF + m);
+  // ops 0, 2 for q < 4, ops 1, 3 for q < 3
+  T af[4][4][5];
 };
+constexpr int kAfdaN = 5;  // samples of each adjusted one-sided derivative
+constexpr int kFsImaging = 1, kFsAfda = 2;  // vi_config.free_surface values
+
+// Bits of the device error word (plan or batch): a bounded wait gave up;
+// a stress value came out non-finite (NaN or Inf in the medium or the
+// state, or an unstable run).
+enum { kErrTimeout = 1, kErrNonFinite = 2 };
 
 __device__ __forceinline__ int strip_x(int i, int nx, int Lx, int Rx) {
   return i < Lx ? i : (i >= nx - Rx ? i - (nx - Rx) + Lx : -1);

@@ -17,9 +17,15 @@
 //    source list (int4 + one amplitude per source) and the receiver list
 //    (int2 per receiver), each block 256-byte aligned.  Larger problems are
 //    rejected with VI_ERR_ARG before anything runs.
-//  * Set-up: the first call on a device (with that device current) looks up
-//    the array's device address once with cudaGetSymbolAddress; later calls
-//    reuse it.  That first call should come before any stream capture.
+//  * Set-up: every call, with the plan's device current, looks up the
+//    array's device address in the current context with
+//    cudaGetSymbolAddress (a table lookup once the module is loaded), so the
+//    address cannot go stale across a cudaDeviceReset or a change of
+//    context.  The first call on a device loads the module that holds the
+//    array: make that first call before any stream capture.
+//  * With sources or receivers, the call stages their lists from its own
+//    stack frame and blocks the host thread on the stream until they are
+//    on the device (cudaStreamSynchronize).
 //  * What must start at zero: the strain planes outside the update region,
 //    which the neighbour averages read and the strain pass never writes.
 //    Each call clears all six planes with cudaMemsetAsync on its stream
@@ -28,7 +34,7 @@
 //    time on one device (different streams, threads or plans) race on it.
 //    Serialize them.
 #include <cstdint>
-#include <mutex>
+#include <string>
 
 #include "plain.cuh"
 #include "plan.cuh"
@@ -39,23 +45,17 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[VI_NOALLOC_SCRA
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 constexpr int kMaxSources = 256;  // host packing buffer on the stack
 
-std::mutex g_mu;
-void *g_addr[kMaxDevices] = {};
-
-// Device address of the static array on `device` (current), looked up once.
-int scratch_address(int device, void **out) {
-  if (device < 0 || device >= kMaxDevices) return set_error(VI_ERR_ARG, "noalloc: device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[device]) {
-    void *ptr = nullptr;
-    const int rc = cuda_check(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress");
-    if (rc) return rc;
-    g_addr[device] = ptr;
-  }
-  *out = g_addr[device];
+// Device address of the static array in the current context.  In host
+// code the array's name is only a host-side stand-in: a kernel given
+// &g_noalloc_scratch would fault or, where the GPU can reach host memory,
+// write the wrong memory, so the address always comes from the runtime.
+int scratch_address(void **out) {
+  void *ptr = nullptr;
+  const int rc = cuda_check(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress");
+  if (rc) return rc;
+  *out = ptr;
   return VI_OK;
 }
 
@@ -69,6 +69,8 @@ int noalloc_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot *s,
   int rc = check_medium(p, m);
   if (rc) return rc;
   if ((rc = check_fields(p, f))) return rc;
+  if (p->cfg.precision == VI_F32C)
+    return set_error(VI_ERR_ARG, "noalloc: the plain step has no compensated FP32 (VI_F32C) form");
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
   const int nsrc = s ? s->nsrc : 0, nrec = s ? s->nrec : 0;
   if (nsrc < 0 || nrec < 0) return set_error(VI_ERR_ARG, "negative source/receiver count");
@@ -102,7 +104,7 @@ int noalloc_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot *s,
   }
   if ((rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice"))) return rc;
   void *base = nullptr;
-  if ((rc = scratch_address(p->device, &base))) return rc;
+  if ((rc = scratch_address(&base))) return rc;
   unsigned char *b = (unsigned char *)base;
   if ((rc = cuda_check(cudaMemsetAsync(b, 0, 6 * np * sizeof(T), st), "noalloc: clear strain planes"))) return rc;
   if (nsrc > 0) {

@@ -9,8 +9,10 @@
 
 namespace vb {
 
+// fs: free-surface kind; under the H-AFDA surface the z derivatives of the
+// four rows below it take the one-sided weights a.af
 template <typename T>
-__global__ void __launch_bounds__(256) k_vel_plain(StepArgs<T> a) {
+__global__ void __launch_bounds__(256) k_vel_plain(const __grid_constant__ StepArgs<T> a, int fs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
   if (i >= a.nx - L || j >= a.nz - L) return;
@@ -24,6 +26,17 @@ __global__ void __launch_bounds__(256) k_vel_plain(StepArgs<T> a) {
     dzxz += a.Dz[k] * (a.sxz[c + (long long)(l - 1) * nx] - a.sxz[c - (long long)l * nx]);
     dxxz += a.Dx[k] * (a.sxz[c + l - 1] - a.sxz[c - l]);
     dzz += a.Dz[k] * (a.szz[c + (long long)l * nx] - a.szz[c - (long long)(l - 1) * nx]);
+  }
+  if (fs == kFsAfda && j < L + 4) {
+    const int q = j - L;
+    dzxz = 0;
+#pragma unroll
+    for (int m = 0; m < kAfdaN; ++m) dzxz += a.af[0][q][m] * a.sxz[(long long)(L + m) * nx + i];
+    if (q < 3) {
+      dzz = 0;
+#pragma unroll
+      for (int m = 0; m < kAfdaN; ++m) dzz += a.af[1][q][m] * a.szz[(long long)(L + 1 + m) * nx + i];
+    }
   }
   const int xs = strip_x(i, nx, a.Lx, a.Rx);
   if (xs >= 0) {
@@ -55,7 +68,7 @@ __global__ void __launch_bounds__(256) k_vel_plain(StepArgs<T> a) {
 // Pass 1 of the stress stage: CPML-corrected rates r and effective SLS rates
 // e into scratch (6 planes of nx*nz: rxx, rzz, rxz, exx, ezz, exz).
 template <typename T, int NSLS>
-__global__ void __launch_bounds__(256) k_strain_plain(StepArgs<T> a, T *scratch) {
+__global__ void __launch_bounds__(256) k_strain_plain(const __grid_constant__ StepArgs<T> a, T *scratch, int fs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + L;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + L;
   if (i >= a.nx - L || j >= a.nz - L) return;
@@ -70,6 +83,19 @@ __global__ void __launch_bounds__(256) k_strain_plain(StepArgs<T> a, T *scratch)
     dzvz += a.Dz[k] * (a.vz[c + (long long)(l - 1) * nx] - a.vz[c - (long long)l * nx]);
     dzvx += a.Dz[k] * (a.vx[c + (long long)l * nx] - a.vx[c - (long long)(l - 1) * nx]);
     dxvz += a.Dx[k] * (a.vz[c + l] - a.vz[c - l + 1]);
+  }
+  if (fs == kFsAfda && j < L + 4) {  // on the surface row the tau_zz = 0 relation sets e_zz
+    const int q = j - L;
+    if (q >= 1) {
+      dzvz = 0;
+#pragma unroll
+      for (int m = 0; m < kAfdaN; ++m) dzvz += a.af[2][q][m] * a.vz[(long long)(L + m) * nx + i];
+    }
+    if (q < 3) {
+      dzvx = 0;
+#pragma unroll
+      for (int m = 0; m < kAfdaN; ++m) dzvx += a.af[3][q][m] * a.vx[(long long)(L + m) * nx + i];
+    }
   }
   const int xs = strip_x(i, nx, a.Lx, a.Rx);
   if (xs >= 0) {
@@ -216,12 +242,13 @@ __global__ void k_receivers(const T *vx, const T *vz, int nx, const int2 *rec, i
   traces[(long long)(nrec + r) * tnt + it] = vz[c];
 }
 
-// Free surface: szz = 0 on row L, stress images above it.
+// Free surface: szz = 0 on row L, and (stress imaging) the images above it.
 template <typename T>
-__global__ void k_mirror(T *szz, T *sxz, int nx) {
+__global__ void k_mirror(T *szz, T *sxz, int nx, int fs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nx) return;
   szz[(long long)L * nx + i] = T(0);
+  if (fs != kFsImaging) return;
 #pragma unroll
   for (int k = 1; k <= L; ++k) szz[(long long)(L - k) * nx + i] = -szz[(long long)(L + k) * nx + i];
 #pragma unroll
@@ -233,21 +260,21 @@ static void plain_step_impl(const StepArgs<T> &a, const PlainExtras<T> &x, int i
                             cudaStream_t st) {
   const dim3 blk(32, 8);
   const dim3 grd((a.nx - 2 * L + 31) / 32, (a.nz - 2 * L + 7) / 8);
-  k_vel_plain<T><<<grd, blk, 0, st>>>(a);
+  k_vel_plain<T><<<grd, blk, 0, st>>>(a, x.fs);
   if (x.nsrc > 0)
     k_sources<T><<<(x.nsrc + 127) / 128, 128, 0, st>>>(a, x.src, x.amp, x.nsrc, x.wavelet,
                                                         x.wnt, it, 0);
   if (x.nrec > 0 && x.traces)
     k_receivers<T><<<(x.nrec + 127) / 128, 128, 0, st>>>(a.vx, a.vz, a.nx, x.rec, x.nrec,
                                                           x.traces, x.tnt, it);
-  k_strain_plain<T, NSLS><<<grd, blk, 0, st>>>(a, x.scratch);
+  k_strain_plain<T, NSLS><<<grd, blk, 0, st>>>(a, x.scratch, x.fs);
   if (x.fs)
     k_surface_rate_plain<T, KIND><<<(a.nx + 127) / 128, 128, 0, st>>>(a, x.scratch);
   k_update_plain<T, KIND, NSLS><<<grd, blk, 0, st>>>(a, x.scratch, x.fs);
   if (x.nsrc > 0)
     k_sources<T><<<(x.nsrc + 127) / 128, 128, 0, st>>>(a, x.src, x.amp, x.nsrc, x.wavelet,
                                                         x.wnt, it, 1);
-  if (x.fs) k_mirror<T><<<(a.nx + 127) / 128, 128, 0, st>>>(a.szz, a.sxz, a.nx);
+  if (x.fs) k_mirror<T><<<(a.nx + 127) / 128, 128, 0, st>>>(a.szz, a.sxz, a.nx, x.fs);
 }
 
 template <typename T>

@@ -23,6 +23,11 @@ struct vi_plan {
   void *tabx = nullptr, *tabz = nullptr;  // 6*nx and 6*nz reals
   void *scratch = nullptr;                // plain path: 6 planes
   void *alt = nullptr;                    // fused path: second v/sigma copy (5 planes)
+  // VI_F32C split step: the stresses' rounding residues (3 bfloat16
+  // planes), part of the plan's state like the CPML memory; slo_valid is
+  // false after a step that did not carry them (they restart from zero)
+  void *slo = nullptr;
+  bool slo_valid = false;
   // source / receiver lists (device, grown on demand)
   void *dsrc = nullptr, *damp = nullptr, *drec = nullptr;
   int src_cap = 0, rec_cap = 0;
@@ -50,6 +55,11 @@ int check_medium(const vi_plan *p, const vi_medium *m);
 // they keep (the new v and sigma, 5 per shot) fit in half the L2.
 inline bool l2_hints_fit(long long kept_bytes, long long l2_bytes) { return 2 * kept_bytes <= l2_bytes; }
 int check_fields(const vi_plan *p, const vi_fields *f);
+// Sets the non-finite bit of the error word `err` when a stress value of
+// the three planes (np cells each) is NaN or infinite (stream-ordered).
+template <typename T>
+int launch_finite_check(const void *sxx, const void *szz, const void *sxz, long long np, int *err, int nsm,
+                        cudaStream_t st);
 // Copies a shot's source / receiver lists to the plan's device buffers.
 template <typename T>
 int stage_shot(vi_plan *p, const vi_shot *s, cudaStream_t st);

@@ -43,6 +43,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "afda.cuh"
 #include "fused_tma.cuh"
 #include "pdl.cuh"
 #include "plan.cuh"
@@ -154,8 +155,9 @@ __device__ __forceinline__ void split_vel_sample(const StepArgs<T> &a, const Fus
 
 // PP: psi read from the input set and written to the output set (TTI);
 // else in place on the input set.  OOP (implies PP): v written to the
-// output state too.
-template <typename T, bool PP, bool OOP, bool HINT>
+// output state too.  AFDA: the grid has the H-AFDA free surface (a
+// separate instantiation, so the others carry none of its registers).
+template <typename T, bool PP, bool OOP, bool HINT, bool AFDA = false>
 __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                int tile) {
   using G = SplitGeom<T>;
@@ -194,6 +196,11 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
       const Q4<T> v = ldg4(a.szz + g + (long long)q * nx);
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
+  }
+  if (AFDA && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface
+    const int qs = gj - L;
+    zxz = afda4<0>(a, qs, [&](int m) { return ldg4(a.sxz + (long long)(L + m) * nx + gi0); });
+    if (qs < 3) zzz = afda4<1>(a, qs, [&](int m) { return ldg4(a.szz + (long long)(L + 1 + m) * nx + gi0); });
   }
   split_vel_finish<T, PP, OOP, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
 }
@@ -261,7 +268,7 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
   const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
-      atomicExch(x.err, 1);
+      atomicOr(x.err, kErrTimeout);
       mbar_wait_bounded(bar, 0, 1u << 22);
     }
     return;
@@ -284,28 +291,34 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
+  if (x.fs == kFsAfda && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L)
+    const int qs = gj - L;
+    zxz = afda4<0>(a, qs, [&](int m) { return lds4(s_sxz + (m + 4) * WX + lx + 4); });
+    if (qs < 3) zzz = afda4<1>(a, qs, [&](int m) { return lds4(s_szz + (m + 5) * WZ + lx); });
+  }
   split_vel_finish<T, PP, false, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
 }
 
 template <typename T, bool PP, bool HINT>
 __global__ void __launch_bounds__(SplitVelTma<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitVelTma<T>::NT)
-    k_split_vel_tma(const StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
+    k_split_vel_tma(const __grid_constant__ StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
   pdl_wait();  // the previous stress pass is complete and visible
   split_vel_tma_tile<T, PP, HINT>(a, x, maps, blockIdx.x);
   split_vel_sample<T>(a, x, blockIdx.x);
 }
 
-template <typename T, bool PP, bool OOP, bool HINT>
+template <typename T, bool PP, bool OOP, bool HINT, bool AFDA>
 __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
-    k_split_vel_ldg(const StepArgs<T> a, const FusedExtras<T> x) {
+    k_split_vel_ldg(const __grid_constant__ StepArgs<T> a, const FusedExtras<T> x) {
   pdl_wait();  // the previous stress pass is complete and visible
-  split_vel_tile<T, PP, OOP, HINT>(a, x, blockIdx.x);
+  split_vel_tile<T, PP, OOP, HINT, AFDA>(a, x, blockIdx.x);
   split_vel_sample<T, OOP>(a, x, blockIdx.x);
 }
 
 // Batched: one tile of one shot per CTA; the step parity selects the shot's
-// argument set (ping-pong buffers for TTI).
-template <typename T, bool PP>
+// argument set (ping-pong buffers for TTI).  AFDA: some shot has the H-AFDA
+// surface (each tile still checks its own shot's kind).
+template <typename T, bool PP, bool AFDA>
 __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitGeom<T>::NT)
     k_split_vel_batch(const BatchDev<T> b, int it) {
   pdl_wait();
@@ -313,17 +326,22 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  split_vel_tile<T, PP, false, false>(b.args[2 * shot + (it & 1)], x, tile);
+  if (AFDA && x.fs == kFsAfda)
+    split_vel_tile<T, PP, false, false, true>(b.args[2 * shot + (it & 1)], x, tile);
+  else
+    split_vel_tile<T, PP, false, false>(b.args[2 * shot + (it & 1)], x, tile);
   split_vel_sample<T>(b.args[2 * shot + (it & 1)], x, tile);
 }
 
 // ------------------------------------------------------------------ stress
 // OOP: sigma, M and psi read from the input state and written to the
 // output one (a.sxx_o.., a.m_o, a.psix_o/psiz_o; the v maps then cover the
-// output velocities); else in place.
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT>
+// output velocities); else in place.  COMP (FP32, in place): sigma is
+// accumulated with its rounding residue (a.slo, two_sum_acc4).
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false>
 __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                   const SplitMaps &maps, int tile) {
+  static_assert(!COMP || (sizeof(T) == 4 && !OOP), "compensated stress: FP32, in place");
   using G = SplitStressGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, SW = G::BW, PB = G::PB;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -368,11 +386,19 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       for (int q = 0; q < 3 * NSLS; ++q) m[q] = ldh4(a.m + q * a.mstride + g, l2_stream_c<HINT>());
     }
   }
+  uint2 lxx{}, lzz{}, lxz{};  // residues of sxx, szz, sxz (COMP)
+  if constexpr (COMP) {
+    if (act) {
+      lxx = ldh_u2(a.slo + g, l2_stream_c<HINT>());
+      lzz = ldh_u2(a.slo + a.slo_plane + g, l2_stream_c<HINT>());
+      lxz = ldh_u2(a.slo + 2 * a.slo_plane + g, l2_stream_c<HINT>());
+    }
+  }
   const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
   const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
-      atomicExch(x.err, 1);
+      atomicOr(x.err, kErrTimeout);
       mbar_wait_bounded(bar, 0, 1u << 22);
     }
     return;
@@ -396,6 +422,11 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       const Q4<T> v = q == 0 ? win4(hvx, 4) : lds4(s_vx + vb + q * SW + 4);
       zvx = fma4(splat4<T>(cq), v, zvx);
     }
+  }
+  if (x.fs == kFsAfda && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L;
+    const int qs = gj - L;              // on the surface row the tau_zz = 0 relation sets e_zz)
+    if (qs >= 1) zvz = afda4<2>(a, qs, [&](int m) { return lds4(s_vz + (m + 4) * SW + lx + 4); });
+    if (qs < 3) zvx = afda4<3>(a, qs, [&](int m) { return lds4(s_vx + (m + 4) * SW + lx + 4); });
   }
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
@@ -460,9 +491,17 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   }
   const Q4<T> c55r{{c55a.v[1], c55a.v[2], c55a.v[3], c55a4}}, c55br{{c55b.v[1], c55b.v[2], c55b.v[3], c55b4}};
   const Q4<T> C55h = mul4(splat4<T>(T(0.25)), add4(add4(add4(c55a, c55r), c55b), c55br));
-  sxx = fma4(dt4, fma4(C11, exx, mul4(C13, ezz)), sxx);
-  szz = fma4(dt4, fma4(C13, exx, mul4(C33, ezz)), szz);
-  sxz = fma4(dt4, mul4(C55h, exz), sxz);
+  // increments (COMP) or the updated stresses
+  Q4<T> ixx, izz, ixz;
+  if constexpr (COMP) {
+    ixx = mul4(dt4, fma4(C11, exx, mul4(C13, ezz)));
+    izz = mul4(dt4, fma4(C13, exx, mul4(C33, ezz)));
+    ixz = mul4(dt4, mul4(C55h, exz));
+  } else {
+    sxx = fma4(dt4, fma4(C11, exx, mul4(C13, ezz)), sxx);
+    szz = fma4(dt4, fma4(C13, exx, mul4(C33, ezz)), szz);
+    sxz = fma4(dt4, mul4(C55h, exz), sxz);
+  }
   if constexpr (NSLS > 0) {
 #pragma unroll
     for (int n = 0; n < NSLS; ++n) {
@@ -481,16 +520,26 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
     if (en.w > TL_EXPLOSIVE) break;
     if (en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
-    add_lane4(sxx, en.x - gi0, dt * x.amp[en.z] * w);
-    add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
+    add_lane4(COMP ? ixx : sxx, en.x - gi0, dt * x.amp[en.z] * w);
+    add_lane4(COMP ? izz : szz, en.x - gi0, dt * x.amp[en.z] * w);
+  }
+  if constexpr (COMP) {
+    two_sum_acc4(sxx, lxx, ixx);
+    two_sum_acc4(szz, lzz, izz);
+    two_sum_acc4(sxz, lxz, ixz);
+    if (surf) lzz = make_uint2(0, 0);
+    sth_u2(a.slo + g, lxx, l2_stream_c<HINT>());
+    sth_u2(a.slo + a.slo_plane + g, lzz, l2_stream_c<HINT>());
+    sth_u2(a.slo + 2 * a.slo_plane + g, lxz, l2_stream_c<HINT>());
   }
   if (surf) szz = Q4<T>{{0, 0, 0, 0}};
+  if (!finite3(sxx, szz, sxz)) atomicOr(x.err, kErrNonFinite);
   T *const osxx = OOP ? a.sxx_o : a.sxx, *const oszz = OOP ? a.szz_o : a.szz, *const osxz = OOP ? a.sxz_o : a.sxz;
   // sigma is re-read by the next velocity pass: keep it in L2
   sth4(osxx + g, sxx, l2_keep_c<HINT>());
   sth4(oszz + g, szz, l2_keep_c<HINT>());
   sth4(osxz + g, sxz, l2_keep_c<HINT>());
-  if (x.fs) {
+  if (x.fs == kFsImaging) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;
     if (k >= 1 && k <= L) {
@@ -508,25 +557,26 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   }
 }
 
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP>
 __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                    const __grid_constant__ SplitMaps maps) {
-  split_stress_tile<T, KIND, NSLS, OOP, HINT>(a, x, maps, blockIdx.x);
+  split_stress_tile<T, KIND, NSLS, OOP, HINT, COMP>(a, x, maps, blockIdx.x);
 }
 
-template <typename T, int KIND, int NSLS>
+template <typename T, int KIND, int NSLS, bool COMP>
 __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress_batch(const BatchDev<T> b, int it) {
   int shot, tile;
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  split_stress_tile<T, KIND, NSLS, false, false>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  // COMP: compensated FP32 shots carry the stress residues, as the unbatched split step
+  split_stress_tile<T, KIND, NSLS, false, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
 // ------------------------------------------------------------------- host
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false>
 static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                            int ntiles, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
@@ -534,37 +584,49 @@ static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const 
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP, HINT>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP, HINT, COMP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP, HINT>, dim3(ntiles), dim3(SG::NT),
+  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP, HINT, COMP>, dim3(ntiles), dim3(SG::NT),
                                (size_t)SG::SMEM, st, pdl, a, x, m),
                     "split stress launch");
 }
 
-// out of place when the caller set the output state (a.sxx_o)
+// out of place when the caller set the output state (a.sxx_o); compensated
+// (FP32, in place) when the caller set the residue planes (a.slo)
 template <typename T, int KIND, int NSLS>
 static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                          int ntiles, cudaStream_t st, bool pdl) {
   // the out-of-place form (the gradient's recompute) always hints
   if (a.sxx_o) return launch_stress_k<T, KIND, NSLS, true, true>(a, x, m, ntiles, st, pdl);
+  if constexpr (sizeof(T) == 4) {
+    if (a.slo)
+      return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true, true>(a, x, m, ntiles, st, pdl)
+                      : launch_stress_k<T, KIND, NSLS, false, false, true>(a, x, m, ntiles, st, pdl);
+  }
   return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true>(a, x, m, ntiles, st, pdl)
                   : launch_stress_k<T, KIND, NSLS, false, false>(a, x, m, ntiles, st, pdl);
+}
+
+template <typename T, bool AFDA>
+static cudaError_t launch_vel_ldg_k(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, cudaStream_t st,
+                                    bool pdl) {
+  using G = SplitGeom<T>;
+  const bool oop = a.vx_o != nullptr, pp = oop || a.psix_o != a.psix || a.psiz_o != a.psiz;
+  return oop        ? launch_pdl(k_split_vel_ldg<T, true, true, true, AFDA>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+         : pp       ? (x.l2hint ? launch_pdl(k_split_vel_ldg<T, true, false, true, AFDA>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+                                : launch_pdl(k_split_vel_ldg<T, true, false, false, AFDA>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x))
+         : x.l2hint ? launch_pdl(k_split_vel_ldg<T, false, false, true, AFDA>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
+                    : launch_pdl(k_split_vel_ldg<T, false, false, false, AFDA>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
 }
 
 template <typename T>
 int launch_split_vel(const StepArgs<T> &a, const FusedExtras<T> &x, int ntiles, cudaStream_t st,
                      bool pdl) {
-  using G = SplitGeom<T>;
-  const bool oop = a.vx_o != nullptr, pp = oop || a.psix_o != a.psix || a.psiz_o != a.psiz;
-  const cudaError_t e =
-      oop         ? launch_pdl(k_split_vel_ldg<T, true, true, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
-      : pp        ? (x.l2hint ? launch_pdl(k_split_vel_ldg<T, true, false, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
-                              : launch_pdl(k_split_vel_ldg<T, true, false, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x))
-      : x.l2hint  ? launch_pdl(k_split_vel_ldg<T, false, false, true>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x)
-                  : launch_pdl(k_split_vel_ldg<T, false, false, false>, dim3(ntiles), dim3(G::NT), 0, st, pdl, a, x);
+  const cudaError_t e = x.fs == kFsAfda ? launch_vel_ldg_k<T, true>(a, x, ntiles, st, pdl)
+                                        : launch_vel_ldg_k<T, false>(a, x, ntiles, st, pdl);
   return cuda_check(e, "split velocity launch");
 }
 
@@ -582,41 +644,50 @@ int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
 }
 
 template <typename T>
-int launch_split_vel_batch(int kind, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
+int launch_split_vel_batch(int kind, bool afda, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
                            bool pdl) {
   using G = SplitGeom<T>;
   if (nitems <= 0) return VI_OK;
+  const bool tti = kind == VI_MEDIUM_TTI;
   const cudaError_t e =
-      kind == VI_MEDIUM_TTI
-          ? launch_pdl(k_split_vel_batch<T, true>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it)
-          : launch_pdl(k_split_vel_batch<T, false>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it);
+      tti  ? (afda ? launch_pdl(k_split_vel_batch<T, true, true>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it)
+                   : launch_pdl(k_split_vel_batch<T, true, false>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it))
+           : (afda ? launch_pdl(k_split_vel_batch<T, false, true>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it)
+                   : launch_pdl(k_split_vel_batch<T, false, false>, dim3(nitems), dim3(G::NT), 0, st, pdl, b, it));
   return cuda_check(e, "batched split velocity launch");
 }
 
-template <typename T, int KIND, int NSLS>
-static int launch_stress_batch(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+template <typename T, int KIND, int NSLS, bool COMP>
+static int launch_stress_batch_k(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_batch<T, KIND, NSLS>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_batch<T, KIND, NSLS, COMP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "batched split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
   if (nitems <= 0) return VI_OK;  // attribute set-up only
-  return cuda_check(launch_pdl(k_split_stress_batch<T, KIND, NSLS>, dim3(nitems), dim3(SG::NT),
+  return cuda_check(launch_pdl(k_split_stress_batch<T, KIND, NSLS, COMP>, dim3(nitems), dim3(SG::NT),
                                (size_t)SG::SMEM, st, pdl, b, it),
                     "batched split stress launch");
 }
 
+template <typename T, int KIND, int NSLS>
+static int launch_stress_batch(bool comp, const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+  if constexpr (sizeof(T) == 4)
+    if (comp) return launch_stress_batch_k<T, KIND, NSLS, true>(b, it, nitems, st, pdl);
+  return launch_stress_batch_k<T, KIND, NSLS, false>(b, it, nitems, st, pdl);
+}
+
 template <typename T>
-int launch_split_stress_batch(int kind, int nsls, const BatchDev<T> &b, int it, int nitems,
+int launch_split_stress_batch(int kind, int nsls, bool comp, const BatchDev<T> &b, int it, int nitems,
                               cudaStream_t st, bool pdl) {
-  if (kind == VI_MEDIUM_TTI) return launch_split_stress_tti_batch<T>(nsls, b, it, nitems, st, pdl);
+  if (kind == VI_MEDIUM_TTI) return launch_split_stress_tti_batch<T>(nsls, comp, b, it, nitems, st, pdl);
 #define VB_CASE(K, N) \
-  if (kind == K && nsls == N) return launch_stress_batch<T, K, N>(b, it, nitems, st, pdl);
+  if (kind == K && nsls == N) return launch_stress_batch<T, K, N>(comp, b, it, nitems, st, pdl);
 #define VB_KIND(K) VB_CASE(K, 0) VB_CASE(K, 1) VB_CASE(K, 2) VB_CASE(K, 3) VB_CASE(K, 4) VB_CASE(K, 5)
   VB_KIND(VI_MEDIUM_ISO)
   VB_KIND(VI_MEDIUM_VTI)
@@ -679,6 +750,26 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     return set_error(VI_ERR_ARG, "pipelined split step does not fit shared memory for this medium");
   if (nsteps == 0) return VI_OK;
   const size_t np = (size_t)c.nx * c.nz;
+  int rc = VI_OK;
+  if constexpr (sizeof(T) == 4) {
+    if (c.precision == VI_F32C) {
+      if (pipelined)
+        return set_error(VI_ERR_ARG, "compensated FP32 (VI_F32C) runs on the one-tile-per-CTA split pair");
+      // compensated stress accumulation: the residue planes live in the plan
+      if (!p->slo) {
+        size_t have = 0;
+        if ((rc = ensure_buffer(p, &p->slo, &have, 3 * np * sizeof(uint16_t)))) return rc;
+        p->slo_valid = false;
+      }
+      if (!p->slo_valid) {
+        if ((rc = cuda_check(cudaMemsetAsync(p->slo, 0, 3 * np * sizeof(uint16_t), st), "zero stress residues")))
+          return rc;
+        p->slo_valid = true;
+      }
+      a.slo = (uint16_t *)p->slo;
+      a.slo_plane = (long long)np;
+    }
+  }
   T *user_m = a.m, *alt_m = nullptr;
   const long long user_ms = a.mstride;
   if (tti && c.nsls > 0) {
@@ -686,7 +777,7 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
     if (!p->alt) {
       const size_t bytes = (5 + 3 * (size_t)c.nsls) * np * sizeof(T);
       size_t have = 0;
-      int rc = ensure_buffer(p, &p->alt, &have, bytes);
+      rc = ensure_buffer(p, &p->alt, &have, bytes);
       if (rc) return rc;
       rc = cuda_check(cudaMemsetAsync(p->alt, 0, bytes, st), "zero alt state");
       if (rc) return rc;
@@ -715,7 +806,7 @@ int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps
   ent.insert(ent.end(), sent.begin(), sent.end());
   int *d_off = nullptr;
   int4 *d_ent = nullptr;
-  int rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent);
+  rc = stage_tile_lists(p, off, ent, st, &d_off, &d_ent);
   if (rc) return rc;
   const int e = sizeof(T);
   SplitMaps ms, mv;
@@ -814,12 +905,12 @@ template int split_steps<float>(vi_plan *, StepArgs<float>, const vi_shot *, int
 template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, int, int,
                                  cudaStream_t, int);
 
-template int launch_split_vel_batch<float>(int, const BatchDev<float> &, int, int, cudaStream_t, bool);
-template int launch_split_vel_batch<double>(int, const BatchDev<double> &, int, int, cudaStream_t,
+template int launch_split_vel_batch<float>(int, bool, const BatchDev<float> &, int, int, cudaStream_t, bool);
+template int launch_split_vel_batch<double>(int, bool, const BatchDev<double> &, int, int, cudaStream_t,
                                             bool);
-template int launch_split_stress_batch<float>(int, int, const BatchDev<float> &, int, int,
+template int launch_split_stress_batch<float>(int, int, bool, const BatchDev<float> &, int, int,
                                               cudaStream_t, bool);
-template int launch_split_stress_batch<double>(int, int, const BatchDev<double> &, int, int,
+template int launch_split_stress_batch<double>(int, int, bool, const BatchDev<double> &, int, int,
                                                cudaStream_t, bool);
 template int launch_split_vel<float>(const StepArgs<float> &, const FusedExtras<float> &, int,
                                      cudaStream_t, bool);

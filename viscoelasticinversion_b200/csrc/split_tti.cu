@@ -17,6 +17,7 @@
 
 #include <cstdint>
 
+#include "afda.cuh"
 #include "pdl.cuh"
 #include "plan.cuh"
 #include "split.cuh"
@@ -29,9 +30,12 @@ namespace vb {
 // 4 cells (gi0.., gj) whose 12-cell x window starts at v-box index wb.  psi
 // is read from the input set and, for the CTA's own cells, written to the
 // output set.
+// fs: the free-surface kind; under the H-AFDA surface the z derivatives of
+// the four rows below it are one-sided (v box row of grid row L + m:
+// wb + (L + m - gj) * BW).
 template <typename T, int BW>
 __device__ __forceinline__ void tti_rates4(const StepArgs<T> &a, const T *s_vx, const T *s_vz,
-                                           int wb, int gi0, int gj, bool own, Q4<T> &rxx,
+                                           int wb, int gi0, int gj, bool own, int fs, Q4<T> &rxx,
                                            Q4<T> &rzz, Q4<T> &rxz) {
   T hvx[12], hvz[12];
   row12s(s_vx + wb, hvx);
@@ -49,6 +53,11 @@ __device__ __forceinline__ void tti_rates4(const StepArgs<T> &a, const T *s_vx, 
       const Q4<T> v = q == 0 ? win4(hvx, 4) : lds4(s_vx + wb + q * BW + 4);
       zvx = fma4(splat4<T>(cq), v, zvx);
     }
+  }
+  if (fs == kFsAfda && gj < L + 4) {  // on the surface row the tau_zz = 0 relation sets e_zz
+    const int qs = gj - L;
+    if (qs >= 1) zvz = afda4<2>(a, qs, [&](int m) { return lds4(s_vz + wb + (L + m - gj) * BW + 4); });
+    if (qs < 3) zvx = afda4<3>(a, qs, [&](int m) { return lds4(s_vx + wb + (L + m - gj) * BW + 4); });
   }
   const int nx = a.nx, nz = a.nz;
   Q4<T> dxvx = dms4(hvx, a.Dx), dxvz = dps4(hvz, a.Dx), dzvz = zvz, dzvx = zvx;
@@ -142,9 +151,11 @@ __device__ __forceinline__ Q4<T> mean4_fwd(const Q4<T> &a, T a4, const Q4<T> &b,
   return mul4(splat4<T>(T(0.25)), add4(add4(add4(a, next4(a, a4)), b), next4(b, b4)));
 }
 
-template <typename T, int NSLS, bool HINT>
+// COMP (FP32): sigma accumulated with its rounding residue (a.slo, two_sum_acc4).
+template <typename T, int NSLS, bool HINT, bool COMP = false>
 __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                       const SplitMaps &maps, int tile) {
+  static_assert(!COMP || sizeof(T) == 4, "compensated stress: FP32");
   using G = SplitTtiGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, BW = G::BW, EW = G::EW, EG = G::EW / 4;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -194,7 +205,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
-      atomicExch(x.err, 1);
+      atomicOr(x.err, kErrTimeout);
       mbar_wait_bounded(bar, 0, 1u << 22);
     }
     return;
@@ -204,7 +215,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   {
     Q4<T> exx = splat4<T>(0), ezz = exx, exz = exx;
     if (act) {
-      tti_rates4<T, BW>(a, s_vx, s_vz, (r + 5) * BW + lx + 4, gi0, gj, true, rxx, rzz, rxz);
+      tti_rates4<T, BW>(a, s_vx, s_vz, (r + 5) * BW + lx + 4, gi0, gj, true, x.fs, rxx, rzz, rxz);
       tti_effective4<T, NSLS>(tau, mxx, mzz, mxz, rxx, rzz, rxz, exx, ezz, exz);
     }
     const int e = (r + 1) * EW + lx + 4;
@@ -216,7 +227,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
     Q4<T> exx = splat4<T>(0), ezz = exx, exz = exx;
     if (ract) {
       Q4<T> qxx, qzz, qxz;
-      tti_rates4<T, BW>(a, s_vx, s_vz, (rr + 4) * BW + rc, rgi0, rgj, false, qxx, qzz, qxz);
+      tti_rates4<T, BW>(a, s_vx, s_vz, (rr + 4) * BW + rc, rgi0, rgj, false, x.fs, qxx, qzz, qxz);
       tti_effective4<T, NSLS>(rtau, qmxx, qmzz, qmxz, qxx, qzz, qxz, exx, ezz, exz);
     }
     const int e = rr * EW + rc;
@@ -265,9 +276,21 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   const Q4<T> C15h = mean4_fwd(c15a, c15a4, c15b, c15b4);
   const Q4<T> C35h = mean4_fwd(c35a, c35a4, c35b, c35b4);
   const Q4<T> C55h = mean4_fwd(c55a, c55a4, c55b, c55b4);
-  sxx = fma4(dt4, fma4(C11, exx, fma4(C13, ezz, mul4(c15a, ebxz))), sxx);
-  szz = fma4(dt4, fma4(C13, exx, fma4(C33, ezz, mul4(c35a, ebxz))), szz);
-  sxz = fma4(dt4, fma4(C55h, exz, fma4(C15h, ebxx, mul4(C35h, ebzz))), sxz);
+  // increments (COMP) or the updated stresses
+  Q4<T> ixx, izz, ixz;
+  uint2 lxx{}, lzz{}, lxz{};
+  if constexpr (COMP) {
+    lxx = ldh_u2(a.slo + g, l2_stream_c<HINT>());
+    lzz = ldh_u2(a.slo + a.slo_plane + g, l2_stream_c<HINT>());
+    lxz = ldh_u2(a.slo + 2 * a.slo_plane + g, l2_stream_c<HINT>());
+    ixx = mul4(dt4, fma4(C11, exx, fma4(C13, ezz, mul4(c15a, ebxz))));
+    izz = mul4(dt4, fma4(C13, exx, fma4(C33, ezz, mul4(c35a, ebxz))));
+    ixz = mul4(dt4, fma4(C55h, exz, fma4(C15h, ebxx, mul4(C35h, ebzz))));
+  } else {
+    sxx = fma4(dt4, fma4(C11, exx, fma4(C13, ezz, mul4(c15a, ebxz))), sxx);
+    szz = fma4(dt4, fma4(C13, exx, fma4(C33, ezz, mul4(c35a, ebxz))), szz);
+    sxz = fma4(dt4, fma4(C55h, exz, fma4(C15h, ebxx, mul4(C35h, ebzz))), sxz);
+  }
   if constexpr (NSLS > 0) {
 #pragma unroll
     for (int n = 0; n < NSLS; ++n) {
@@ -287,15 +310,25 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
     if (en.w > TL_EXPLOSIVE) break;
     if (en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
     const T w = x.it < x.wnt ? x.wavelet[(long long)en.z * x.wnt + x.it] : T(0);
-    add_lane4(sxx, en.x - gi0, dt * x.amp[en.z] * w);
-    add_lane4(szz, en.x - gi0, dt * x.amp[en.z] * w);
+    add_lane4(COMP ? ixx : sxx, en.x - gi0, dt * x.amp[en.z] * w);
+    add_lane4(COMP ? izz : szz, en.x - gi0, dt * x.amp[en.z] * w);
+  }
+  if constexpr (COMP) {
+    two_sum_acc4(sxx, lxx, ixx);
+    two_sum_acc4(szz, lzz, izz);
+    two_sum_acc4(sxz, lxz, ixz);
+    if (surf) lzz = make_uint2(0, 0);
+    sth_u2(a.slo + g, lxx, l2_stream_c<HINT>());
+    sth_u2(a.slo + a.slo_plane + g, lzz, l2_stream_c<HINT>());
+    sth_u2(a.slo + 2 * a.slo_plane + g, lxz, l2_stream_c<HINT>());
   }
   if (surf) szz = splat4<T>(0);
+  if (!finite3(sxx, szz, sxz)) atomicOr(x.err, kErrNonFinite);
   // sigma is re-read by the next velocity pass: keep it in L2
   sth4(a.sxx + g, sxx, l2_keep_c<HINT>());
   sth4(a.szz + g, szz, l2_keep_c<HINT>());
   sth4(a.sxz + g, sxz, l2_keep_c<HINT>());
-  if (x.fs) {
+  if (x.fs == kFsImaging) {
     // stress images: szz(L-k) = -szz(L+k), k = 1..4; sxz(L-1-k) = -sxz(L+k), k = 0..3
     const int k = gj - L;
     if (k >= 1 && k <= L) stg4(a.szz + (long long)(L - k) * nx + gi0, mul4(splat4<T>(T(-1)), szz));
@@ -303,26 +336,27 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   }
 }
 
-template <typename T, int NSLS, bool HINT>
+template <typename T, int NSLS, bool HINT, bool COMP>
 __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
     k_split_stress_tti(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                        const __grid_constant__ SplitMaps maps) {
-  split_stress_tti_tile<T, NSLS, HINT>(a, x, maps, blockIdx.x);
+  split_stress_tti_tile<T, NSLS, HINT, COMP>(a, x, maps, blockIdx.x);
 }
 
 // Batched: one tile of one shot per CTA; the step parity selects the
 // shot's M / psi buffers.
-template <typename T, int NSLS>
+template <typename T, int NSLS, bool COMP>
 __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
     k_split_stress_tti_batch(const BatchDev<T> b, int it) {
   int shot, tile;
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  split_stress_tti_tile<T, NSLS, false>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  // COMP: compensated FP32 shots carry the stress residues, as the unbatched split step
+  split_stress_tti_tile<T, NSLS, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
-template <typename T, int NSLS, bool HINT>
+template <typename T, int NSLS, bool HINT, bool COMP = false>
 static int launch_tti_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
                         cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
@@ -330,19 +364,25 @@ static int launch_tti_k(const StepArgs<T> &a, const FusedExtras<T> &x, const Spl
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti<T, NSLS, HINT>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti<T, NSLS, HINT, COMP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split TTI stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress_tti<T, NSLS, HINT>, dim3(ntiles), dim3(G::NT),
+  return cuda_check(launch_pdl(k_split_stress_tti<T, NSLS, HINT, COMP>, dim3(ntiles), dim3(G::NT),
                                (size_t)G::SMEM, st, pdl, a, x, m),
                     "split TTI stress launch");
 }
 
+// compensated (FP32) when the caller set the residue planes (a.slo)
 template <typename T, int NSLS>
 static int launch_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
                       cudaStream_t st, bool pdl) {
+  if constexpr (sizeof(T) == 4) {
+    if (a.slo)
+      return x.l2hint ? launch_tti_k<T, NSLS, true, true>(a, x, m, ntiles, st, pdl)
+                      : launch_tti_k<T, NSLS, false, true>(a, x, m, ntiles, st, pdl);
+  }
   return x.l2hint ? launch_tti_k<T, NSLS, true>(a, x, m, ntiles, st, pdl)
                   : launch_tti_k<T, NSLS, false>(a, x, m, ntiles, st, pdl);
 }
@@ -361,41 +401,48 @@ int launch_split_stress_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const
   }
 }
 
-template <typename T, int NSLS>
-static int launch_tti_batch(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+template <typename T, int NSLS, bool COMP>
+static int launch_tti_batch_k(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti_batch<T, NSLS>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti_batch<T, NSLS, COMP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "batched split TTI stress smem attribute");
     attr_set |= 1ULL << dev;
   }
   if (nitems <= 0) return VI_OK;  // attribute set-up only
-  return cuda_check(launch_pdl(k_split_stress_tti_batch<T, NSLS>, dim3(nitems), dim3(G::NT),
+  return cuda_check(launch_pdl(k_split_stress_tti_batch<T, NSLS, COMP>, dim3(nitems), dim3(G::NT),
                                (size_t)G::SMEM, st, pdl, b, it),
                     "batched split TTI stress launch");
 }
 
+template <typename T, int NSLS>
+static int launch_tti_batch(bool comp, const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+  if constexpr (sizeof(T) == 4)
+    if (comp) return launch_tti_batch_k<T, NSLS, true>(b, it, nitems, st, pdl);
+  return launch_tti_batch_k<T, NSLS, false>(b, it, nitems, st, pdl);
+}
+
 template <typename T>
-int launch_split_stress_tti_batch(int nsls, const BatchDev<T> &b, int it, int nitems,
+int launch_split_stress_tti_batch(int nsls, bool comp, const BatchDev<T> &b, int it, int nitems,
                                   cudaStream_t st, bool pdl) {
   switch (nsls) {
-    case 0: return launch_tti_batch<T, 0>(b, it, nitems, st, pdl);
-    case 1: return launch_tti_batch<T, 1>(b, it, nitems, st, pdl);
-    case 2: return launch_tti_batch<T, 2>(b, it, nitems, st, pdl);
-    case 3: return launch_tti_batch<T, 3>(b, it, nitems, st, pdl);
-    case 4: return launch_tti_batch<T, 4>(b, it, nitems, st, pdl);
-    case 5: return launch_tti_batch<T, 5>(b, it, nitems, st, pdl);
+    case 0: return launch_tti_batch<T, 0>(comp, b, it, nitems, st, pdl);
+    case 1: return launch_tti_batch<T, 1>(comp, b, it, nitems, st, pdl);
+    case 2: return launch_tti_batch<T, 2>(comp, b, it, nitems, st, pdl);
+    case 3: return launch_tti_batch<T, 3>(comp, b, it, nitems, st, pdl);
+    case 4: return launch_tti_batch<T, 4>(comp, b, it, nitems, st, pdl);
+    case 5: return launch_tti_batch<T, 5>(comp, b, it, nitems, st, pdl);
     default: return set_error(VI_ERR_ARG, "nsls must be 0..5");
   }
 }
 
-template int launch_split_stress_tti_batch<float>(int, const BatchDev<float> &, int, int,
+template int launch_split_stress_tti_batch<float>(int, bool, const BatchDev<float> &, int, int,
                                                   cudaStream_t, bool);
-template int launch_split_stress_tti_batch<double>(int, const BatchDev<double> &, int, int,
+template int launch_split_stress_tti_batch<double>(int, bool, const BatchDev<double> &, int, int,
                                                    cudaStream_t, bool);
 template int launch_split_stress_tti<float>(const StepArgs<float> &, const FusedExtras<float> &,
                                             const SplitMaps &, int, cudaStream_t, bool);

@@ -50,11 +50,16 @@ template <typename T>
 __device__ __forceinline__ T lane4(const Q4<T> &q, int k) {
   return k == 0 ? q.v[0] : k == 1 ? q.v[1] : k == 2 ? q.v[2] : q.v[3];
 }
+// q[k] += d as one rounded addition (never contracted with the product
+// that formed d), so every kernel instantiation that inlines it adds a
+// source term with the same bits
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 template <typename T>
 __device__ __forceinline__ void add_lane4(Q4<T> &q, int k, T d) {
 #pragma unroll
   for (int i = 0; i < 4; ++i)
-    if (i == k) q.v[i] += d;
+    if (i == k) q.v[i] = add_rn(q.v[i], d);
 }
 // ---- L2 eviction priority hints (createpolicy + .L2::cache_hint): lines
 // re-read by the other pass of the step are kept (evict_last), lines that
@@ -220,6 +225,52 @@ __device__ __forceinline__ Q4<double> add4(const Q4<double> &a, const Q4<double>
 template <typename T>
 __device__ __forceinline__ Q4<T> sub4(const Q4<T> &a, const Q4<T> &b) {  // a - b, exact as one rounding
   return fma4(b, splat4<T>(T(-1)), a);
+}
+// ---- compensated accumulation of a 4-cell group (FP32 with a bfloat16
+// residue per cell).  A float sigma updated 4000 times loses the low bits
+// of every increment, and the part of that rounding noise that has no
+// divergence never radiates away: it stays in sigma as a static field.
+// Carrying each cell's rounding error in a residue plane and folding it
+// into the next increment removes that drift.  hi + lo += d: x = d + lo,
+// s = hi + x exactly split into s and its error e by Knuth's two-sum
+// (six round-to-nearest additions, valid whatever the magnitudes), then
+// hi = s and lo = e rounded to bfloat16 (8 more bits than the float).
+__device__ __forceinline__ Q4<float> bf16x4_to_f32(uint2 u) {
+  return {{__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u), __uint_as_float(u.y << 16),
+           __uint_as_float(u.y & 0xffff0000u)}};
+}
+__device__ __forceinline__ uint32_t f32x2_to_bf16x2(float lo, float hi) {  // round to nearest even
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+__device__ __forceinline__ uint2 f32_to_bf16x4(const Q4<float> &q) {
+  return make_uint2(f32x2_to_bf16x2(q.v[0], q.v[1]), f32x2_to_bf16x2(q.v[2], q.v[3]));
+}
+__device__ __forceinline__ void two_sum_acc4(Q4<float> &hi, uint2 &lo, const Q4<float> &d) {
+  const Q4<float> x = add4(d, bf16x4_to_f32(lo));
+  const Q4<float> s = add4(hi, x);
+  const Q4<float> bp = sub4(s, hi);
+  const Q4<float> e = add4(sub4(hi, sub4(s, bp)), sub4(x, bp));
+  hi = s;
+  lo = f32_to_bf16x4(e);
+}
+__device__ __forceinline__ uint2 ldh_u2(const uint16_t *p, uint64_t pol) {
+  uint2 q;
+  asm volatile("ld.global.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(q.x), "=r"(q.y) : "l"(p), "l"(pol));
+  return q;
+}
+__device__ __forceinline__ void sth_u2(uint16_t *p, uint2 q, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.u32 [%0], {%1, %2}, %3;" ::"l"(p), "r"(q.x), "r"(q.y), "l"(pol)
+               : "memory");
+}
+// true when the 12 values of three groups are finite (a NaN or an
+// infinity anywhere makes their sum non-finite; so does an overflowing sum,
+// which is an unstable run as well)
+template <typename T>
+__device__ __forceinline__ bool finite3(const Q4<T> &a, const Q4<T> &b, const Q4<T> &c) {
+  const Q4<T> s = add4(add4(a, b), c);
+  return isfinite((s.v[0] + s.v[1]) + (s.v[2] + s.v[3]));
 }
 // window of 4 consecutive values of a 12-value row, starting at o
 template <typename T>

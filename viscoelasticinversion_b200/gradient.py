@@ -139,6 +139,32 @@ def thomsen_gradient(grad: torch.Tensor, vp: torch.Tensor, vs: torch.Tensor, rho
     return out
 
 
+TTI_PARAMETERS = ("vp", "vs", "rho", "qinv", "eps", "delta", "theta")
+
+
+def tti_gradient(grad: torch.Tensor, vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tensor,
+                 eps: torch.Tensor | None = None, delta: torch.Tensor | None = None,
+                 theta: torch.Tensor | None = None, tau_scale: float = 0.0, stream=None) -> torch.Tensor:
+    """[7, nz, nx] float64: dJ/d(vp, vs, rho, 1/Q, epsilon, delta, theta) of
+    a TTI medium (TTI_PARAMETERS order) from the stiffness gradient of
+    vi_gradient, through Thomsen's law tilted by theta (the map of
+    medium_from_velocity / media.bond_rotate)."""
+    np_ = grad.shape[1] * grad.shape[2]
+    out = torch.empty(7, grad.shape[1], grad.shape[2], dtype=torch.float64, device=grad.device)
+
+    def p(t):
+        if t is None:
+            return None
+        if t.dtype != torch.float64 or not t.is_contiguous() or t.numel() != np_:
+            raise ValueError("parameter planes must be contiguous float64 [nz, nx]")
+        return t.data_ptr()
+
+    with torch.cuda.device(grad.device):
+        check(lib().vi_gradient_tti(np_, grad.data_ptr(), p(vp), p(vs), p(rho), p(eps), p(delta), p(theta),
+                                    float(tau_scale), out.data_ptr(), _stream_handle(stream)))
+    return out
+
+
 def shard(nshots: int, rank: int, world: int) -> list[int]:
     """Shots of this rank: round robin, so uneven shot costs spread."""
     return list(range(rank, nshots, world))

@@ -208,7 +208,7 @@ class Workload:
     kind: str                    # "iso" | "vti" | "tti"
     medium: dict                 # name -> float64 array [nz, nx]
     taus: np.ndarray             # τ_n (empty for elastic)
-    free_surface: bool
+    free_surface: int  # 0/False none, 1/True stress imaging, 2 H-AFDA
     pml: int
     pml_vmax: float
     pml_alpha_max: float

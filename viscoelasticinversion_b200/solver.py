@@ -16,9 +16,12 @@ import torch
 
 from . import _abi
 from ._abi import (ViConfig, ViFields, ViMedium, ViReceiver, ViShot, ViSource, check, lib,
-                   MEDIUM_KINDS, VI_F32, VI_F64)
+                   MEDIUM_KINDS, PRECISIONS, VI_F32, VI_F64)
 
 MEDIUM_NAMES = ("rho", "c11", "c13", "c15", "c33", "c35", "c55", "tau")
+# vi_config.free_surface: 1 = stress imaging (CPML.jl:366-393), 2 = H-AFDA
+# one-sided derivatives (free-surface-kernels.jl, Stencil.jl:52-105)
+FREE_SURFACE_IMAGING, FREE_SURFACE_HAFDA = 1, 2
 
 
 @dataclass
@@ -44,11 +47,12 @@ def make_config(nx, nz, dx, dz, dt, kind="iso", precision="f32", taus=(), free_s
     c = ViConfig()
     c.nx, c.nz, c.dx, c.dz, c.dt = int(nx), int(nz), float(dx), float(dz), float(dt)
     c.medium = MEDIUM_KINDS[kind]
-    c.precision = VI_F64 if precision == "f64" else VI_F32
+    c.precision = PRECISIONS[precision]
     c.nsls = len(taus)
     for n, t in enumerate(taus):
         c.tau_sls[n] = float(t)
-    c.free_surface = int(bool(free_surface))
+    # False / 0: none; True / 1: stress imaging; 2 (FREE_SURFACE_HAFDA): H-AFDA
+    c.free_surface = FREE_SURFACE_HAFDA if free_surface == FREE_SURFACE_HAFDA else int(bool(free_surface))
     if cpml is not None and cpml.thickness > 0:
         c.pml_thickness = cpml.thickness
         c.pml_left, c.pml_right = int(cpml.left), int(cpml.right)
