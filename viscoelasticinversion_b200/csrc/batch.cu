@@ -272,7 +272,7 @@ static int launch_steps(vi_batch *b, const BatchDev<T> &bd, int form, int it0, i
       // at entry (programmatic dependent launch), as the one-shot pair does
       rc = launch_split_vel_batch<T>(b->kind, b->afda, bd, it, nitems, st, it > it0);
       if (!rc)
-        rc = launch_split_stress_batch<T>(b->kind, b->nsls, b->precision == VI_F32C, bd, it, nitems, st, true);
+        rc = launch_split_stress_batch<T>(b->kind, b->nsls, b->precision == VI_F32C, b->afda, bd, it, nitems, st, true);
     } else {
       rc = launch_fused_tma_batch<T>(b->kind, b->nsls, bd, it, nitems, b->nsm, form == kFormTwoStage, st);
     }
@@ -392,7 +392,7 @@ static int tune(vi_batch *b, cudaStream_t st) {
 template <typename T>
 static int set_up_form(vi_batch *b, const BatchDev<T> &bd, int form, cudaStream_t st) {
   if (form == kFormSplit)
-    return launch_split_stress_batch<T>(b->kind, b->nsls, b->precision == VI_F32C, bd, 0, 0, st, false);
+    return launch_split_stress_batch<T>(b->kind, b->nsls, b->precision == VI_F32C, b->afda, bd, 0, 0, st, false);
   return launch_fused_tma_batch<T>(b->kind, b->nsls, bd, 0, 0, b->nsm, form == kFormTwoStage, st);
 }
 

@@ -230,7 +230,7 @@ struct SplitVelTma {
   static_assert((WX * TZ * sizeof(T)) % 16 == 0 && (WX * HZ * sizeof(T)) % 16 == 0, "16-byte boxes");
 };
 
-template <typename T, bool PP, bool HINT>
+template <typename T, bool PP, bool HINT, bool AFDA>
 __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                    const SplitMaps &maps, int tile) {
   using G = SplitVelTma<T>;
@@ -291,7 +291,7 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
-  if (x.fs == kFsAfda && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L)
+  if (AFDA && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L)
     const int qs = gj - L;
     zxz = afda4<0>(a, qs, [&](int m) { return lds4(s_sxz + (m + 4) * WX + lx + 4); });
     if (qs < 3) zzz = afda4<1>(a, qs, [&](int m) { return lds4(s_szz + (m + 5) * WZ + lx); });
@@ -299,11 +299,13 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
   split_vel_finish<T, PP, false, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
 }
 
-template <typename T, bool PP, bool HINT>
+// AFDA: the grid has the H-AFDA free surface (a separate instantiation,
+// so the others carry none of its code)
+template <typename T, bool PP, bool HINT, bool AFDA>
 __global__ void __launch_bounds__(SplitVelTma<T>::NT, (sizeof(T) == 4 ? 1024 : 512) / SplitVelTma<T>::NT)
     k_split_vel_tma(const __grid_constant__ StepArgs<T> a, const FusedExtras<T> x, const __grid_constant__ SplitMaps maps) {
   pdl_wait();  // the previous stress pass is complete and visible
-  split_vel_tma_tile<T, PP, HINT>(a, x, maps, blockIdx.x);
+  split_vel_tma_tile<T, PP, HINT, AFDA>(a, x, maps, blockIdx.x);
   split_vel_sample<T>(a, x, blockIdx.x);
 }
 
@@ -338,7 +340,7 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
 // output one (a.sxx_o.., a.m_o, a.psix_o/psiz_o; the v maps then cover the
 // output velocities); else in place.  COMP (FP32, in place): sigma is
 // accumulated with its rounding residue (a.slo, two_sum_acc4).
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false, bool AFDA = false>
 __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                   const SplitMaps &maps, int tile) {
   static_assert(!COMP || (sizeof(T) == 4 && !OOP), "compensated stress: FP32, in place");
@@ -423,7 +425,7 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       zvx = fma4(splat4<T>(cq), v, zvx);
     }
   }
-  if (x.fs == kFsAfda && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L;
+  if (AFDA && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L;
     const int qs = gj - L;              // on the surface row the tau_zz = 0 relation sets e_zz)
     if (qs >= 1) zvz = afda4<2>(a, qs, [&](int m) { return lds4(s_vz + (m + 4) * SW + lx + 4); });
     if (qs < 3) zvx = afda4<3>(a, qs, [&](int m) { return lds4(s_vx + (m + 4) * SW + lx + 4); });
@@ -557,26 +559,30 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   }
 }
 
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP, bool AFDA>
 __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                    const __grid_constant__ SplitMaps maps) {
-  split_stress_tile<T, KIND, NSLS, OOP, HINT, COMP>(a, x, maps, blockIdx.x);
+  split_stress_tile<T, KIND, NSLS, OOP, HINT, COMP, AFDA>(a, x, maps, blockIdx.x);
 }
 
-template <typename T, int KIND, int NSLS, bool COMP>
+template <typename T, int KIND, int NSLS, bool COMP, bool AFDA>
 __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
     k_split_stress_batch(const BatchDev<T> b, int it) {
   int shot, tile;
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  // COMP: compensated FP32 shots carry the stress residues, as the unbatched split step
-  split_stress_tile<T, KIND, NSLS, false, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  // COMP: compensated FP32 shots carry the stress residues, as the unbatched
+  // split step; AFDA: some shot has the H-AFDA surface
+  if (AFDA && x.fs == kFsAfda)
+    split_stress_tile<T, KIND, NSLS, false, false, COMP, true>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  else
+    split_stress_tile<T, KIND, NSLS, false, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
 // ------------------------------------------------------------------- host
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false, bool AFDA = false>
 static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
                            int ntiles, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
@@ -584,12 +590,12 @@ static int launch_stress_k(const StepArgs<T> &a, const FusedExtras<T> &x, const 
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP, HINT, COMP>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress<T, KIND, NSLS, OOP, HINT, COMP, AFDA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP, HINT, COMP>, dim3(ntiles), dim3(SG::NT),
+  return cuda_check(launch_pdl(k_split_stress<T, KIND, NSLS, OOP, HINT, COMP, AFDA>, dim3(ntiles), dim3(SG::NT),
                                (size_t)SG::SMEM, st, pdl, a, x, m),
                     "split stress launch");
 }
@@ -602,10 +608,17 @@ static int launch_stress(const StepArgs<T> &a, const FusedExtras<T> &x, const Sp
   // the out-of-place form (the gradient's recompute) always hints
   if (a.sxx_o) return launch_stress_k<T, KIND, NSLS, true, true>(a, x, m, ntiles, st, pdl);
   if constexpr (sizeof(T) == 4) {
-    if (a.slo)
+    if (a.slo) {
+      if (x.fs == kFsAfda)
+        return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true, true, true>(a, x, m, ntiles, st, pdl)
+                        : launch_stress_k<T, KIND, NSLS, false, false, true, true>(a, x, m, ntiles, st, pdl);
       return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true, true>(a, x, m, ntiles, st, pdl)
                       : launch_stress_k<T, KIND, NSLS, false, false, true>(a, x, m, ntiles, st, pdl);
+    }
   }
+  if (x.fs == kFsAfda)
+    return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true, false, true>(a, x, m, ntiles, st, pdl)
+                    : launch_stress_k<T, KIND, NSLS, false, false, false, true>(a, x, m, ntiles, st, pdl);
   return x.l2hint ? launch_stress_k<T, KIND, NSLS, false, true>(a, x, m, ntiles, st, pdl)
                   : launch_stress_k<T, KIND, NSLS, false, false>(a, x, m, ntiles, st, pdl);
 }
@@ -657,37 +670,41 @@ int launch_split_vel_batch(int kind, bool afda, const BatchDev<T> &b, int it, in
   return cuda_check(e, "batched split velocity launch");
 }
 
-template <typename T, int KIND, int NSLS, bool COMP>
+template <typename T, int KIND, int NSLS, bool COMP, bool AFDA>
 static int launch_stress_batch_k(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
   using SG = SplitStressGeom<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_batch<T, KIND, NSLS, COMP>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_batch<T, KIND, NSLS, COMP, AFDA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SG::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "batched split stress smem attribute");
     attr_set |= 1ULL << dev;
   }
   if (nitems <= 0) return VI_OK;  // attribute set-up only
-  return cuda_check(launch_pdl(k_split_stress_batch<T, KIND, NSLS, COMP>, dim3(nitems), dim3(SG::NT),
+  return cuda_check(launch_pdl(k_split_stress_batch<T, KIND, NSLS, COMP, AFDA>, dim3(nitems), dim3(SG::NT),
                                (size_t)SG::SMEM, st, pdl, b, it),
                     "batched split stress launch");
 }
 
 template <typename T, int KIND, int NSLS>
-static int launch_stress_batch(bool comp, const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+static int launch_stress_batch(bool comp, bool afda, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
+                               bool pdl) {
   if constexpr (sizeof(T) == 4)
-    if (comp) return launch_stress_batch_k<T, KIND, NSLS, true>(b, it, nitems, st, pdl);
-  return launch_stress_batch_k<T, KIND, NSLS, false>(b, it, nitems, st, pdl);
+    if (comp)
+      return afda ? launch_stress_batch_k<T, KIND, NSLS, true, true>(b, it, nitems, st, pdl)
+                  : launch_stress_batch_k<T, KIND, NSLS, true, false>(b, it, nitems, st, pdl);
+  return afda ? launch_stress_batch_k<T, KIND, NSLS, false, true>(b, it, nitems, st, pdl)
+              : launch_stress_batch_k<T, KIND, NSLS, false, false>(b, it, nitems, st, pdl);
 }
 
 template <typename T>
-int launch_split_stress_batch(int kind, int nsls, bool comp, const BatchDev<T> &b, int it, int nitems,
+int launch_split_stress_batch(int kind, int nsls, bool comp, bool afda, const BatchDev<T> &b, int it, int nitems,
                               cudaStream_t st, bool pdl) {
-  if (kind == VI_MEDIUM_TTI) return launch_split_stress_tti_batch<T>(nsls, comp, b, it, nitems, st, pdl);
+  if (kind == VI_MEDIUM_TTI) return launch_split_stress_tti_batch<T>(nsls, comp, afda, b, it, nitems, st, pdl);
 #define VB_CASE(K, N) \
-  if (kind == K && nsls == N) return launch_stress_batch<T, K, N>(comp, b, it, nitems, st, pdl);
+  if (kind == K && nsls == N) return launch_stress_batch<T, K, N>(comp, afda, b, it, nitems, st, pdl);
 #define VB_KIND(K) VB_CASE(K, 0) VB_CASE(K, 1) VB_CASE(K, 2) VB_CASE(K, 3) VB_CASE(K, 4) VB_CASE(K, 5)
   VB_KIND(VI_MEDIUM_ISO)
   VB_KIND(VI_MEDIUM_VTI)
@@ -711,28 +728,35 @@ bool split_eligible(const vi_plan *p, const StepArgs<T> &a) {
   return true;
 }
 
-template <typename T>
-static int launch_vel_tma(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
-                          int ntiles, cudaStream_t st, bool pdl) {
+template <typename T, bool AFDA>
+static int launch_vel_tma_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                            int ntiles, cudaStream_t st, bool pdl) {
   using G = SplitVelTma<T>;
   const bool pp = a.psix_o != a.psix || a.psiz_o != a.psiz;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    for (auto k : {k_split_vel_tma<T, true, true>, k_split_vel_tma<T, false, true>, k_split_vel_tma<T, true, false>,
-                   k_split_vel_tma<T, false, false>}) {
+    for (auto k : {k_split_vel_tma<T, true, true, AFDA>, k_split_vel_tma<T, false, true, AFDA>,
+                   k_split_vel_tma<T, true, false, AFDA>, k_split_vel_tma<T, false, false, AFDA>}) {
       const cudaError_t ea = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
       if (ea != cudaSuccess) return cuda_check(ea, "split velocity (TMA) smem attribute");
     }
     attr_set |= 1ULL << dev;
   }
   const cudaError_t e =
-      pp ? (x.l2hint ? launch_pdl(k_split_vel_tma<T, true, true>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
-                     : launch_pdl(k_split_vel_tma<T, true, false>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m))
-         : (x.l2hint ? launch_pdl(k_split_vel_tma<T, false, true>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
-                     : launch_pdl(k_split_vel_tma<T, false, false>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m));
+      pp ? (x.l2hint ? launch_pdl(k_split_vel_tma<T, true, true, AFDA>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
+                     : launch_pdl(k_split_vel_tma<T, true, false, AFDA>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m))
+         : (x.l2hint ? launch_pdl(k_split_vel_tma<T, false, true, AFDA>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m)
+                     : launch_pdl(k_split_vel_tma<T, false, false, AFDA>, dim3(ntiles), dim3(G::NT), (size_t)G::SMEM, st, pdl, a, x, m));
   return cuda_check(e, "split velocity (TMA) launch");
+}
+
+template <typename T>
+static int launch_vel_tma(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m,
+                          int ntiles, cudaStream_t st, bool pdl) {
+  return x.fs == kFsAfda ? launch_vel_tma_k<T, true>(a, x, m, ntiles, st, pdl)
+                         : launch_vel_tma_k<T, false>(a, x, m, ntiles, st, pdl);
 }
 
 template <typename T>
@@ -908,9 +932,9 @@ template int split_steps<double>(vi_plan *, StepArgs<double>, const vi_shot *, i
 template int launch_split_vel_batch<float>(int, bool, const BatchDev<float> &, int, int, cudaStream_t, bool);
 template int launch_split_vel_batch<double>(int, bool, const BatchDev<double> &, int, int, cudaStream_t,
                                             bool);
-template int launch_split_stress_batch<float>(int, int, bool, const BatchDev<float> &, int, int,
+template int launch_split_stress_batch<float>(int, int, bool, bool, const BatchDev<float> &, int, int,
                                               cudaStream_t, bool);
-template int launch_split_stress_batch<double>(int, int, bool, const BatchDev<double> &, int, int,
+template int launch_split_stress_batch<double>(int, int, bool, bool, const BatchDev<double> &, int, int,
                                                cudaStream_t, bool);
 template int launch_split_vel<float>(const StepArgs<float> &, const FusedExtras<float> &, int,
                                      cudaStream_t, bool);

@@ -74,12 +74,13 @@ int launch_split_stress(int kind, const StepArgs<T> &a, const FusedExtras<T> &x,
 template <typename T>
 int launch_split_vel_batch(int kind, bool afda, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
                            bool pdl);
-// comp: the shots are compensated FP32 (VI_F32C: stress residues in args.slo)
+// comp: the shots are compensated FP32 (VI_F32C: stress residues in
+// args.slo); afda: some shot has the H-AFDA free surface
 template <typename T>
-int launch_split_stress_batch(int kind, int nsls, bool comp, const BatchDev<T> &b, int it, int nitems,
+int launch_split_stress_batch(int kind, int nsls, bool comp, bool afda, const BatchDev<T> &b, int it, int nitems,
                               cudaStream_t st, bool pdl);
 template <typename T>
-int launch_split_stress_tti_batch(int nsls, bool comp, const BatchDev<T> &b, int it, int nitems,
+int launch_split_stress_tti_batch(int nsls, bool comp, bool afda, const BatchDev<T> &b, int it, int nitems,
                                   cudaStream_t st, bool pdl);
 
 // TTI stress pass: reads M (a.m) and psi (a.psix/psiz) of the tile and its

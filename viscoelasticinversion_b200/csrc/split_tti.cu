@@ -30,12 +30,12 @@ namespace vb {
 // 4 cells (gi0.., gj) whose 12-cell x window starts at v-box index wb.  psi
 // is read from the input set and, for the CTA's own cells, written to the
 // output set.
-// fs: the free-surface kind; under the H-AFDA surface the z derivatives of
+// AFDA: the grid has the H-AFDA surface, under which the z derivatives of
 // the four rows below it are one-sided (v box row of grid row L + m:
 // wb + (L + m - gj) * BW).
-template <typename T, int BW>
+template <typename T, int BW, bool AFDA>
 __device__ __forceinline__ void tti_rates4(const StepArgs<T> &a, const T *s_vx, const T *s_vz,
-                                           int wb, int gi0, int gj, bool own, int fs, Q4<T> &rxx,
+                                           int wb, int gi0, int gj, bool own, Q4<T> &rxx,
                                            Q4<T> &rzz, Q4<T> &rxz) {
   T hvx[12], hvz[12];
   row12s(s_vx + wb, hvx);
@@ -54,7 +54,7 @@ __device__ __forceinline__ void tti_rates4(const StepArgs<T> &a, const T *s_vx, 
       zvx = fma4(splat4<T>(cq), v, zvx);
     }
   }
-  if (fs == kFsAfda && gj < L + 4) {  // on the surface row the tau_zz = 0 relation sets e_zz
+  if (AFDA && gj < L + 4) {  // on the surface row the tau_zz = 0 relation sets e_zz
     const int qs = gj - L;
     if (qs >= 1) zvz = afda4<2>(a, qs, [&](int m) { return lds4(s_vz + wb + (L + m - gj) * BW + 4); });
     if (qs < 3) zvx = afda4<3>(a, qs, [&](int m) { return lds4(s_vx + wb + (L + m - gj) * BW + 4); });
@@ -152,7 +152,7 @@ __device__ __forceinline__ Q4<T> mean4_fwd(const Q4<T> &a, T a4, const Q4<T> &b,
 }
 
 // COMP (FP32): sigma accumulated with its rounding residue (a.slo, two_sum_acc4).
-template <typename T, int NSLS, bool HINT, bool COMP = false>
+template <typename T, int NSLS, bool HINT, bool COMP = false, bool AFDA = false>
 __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                       const SplitMaps &maps, int tile) {
   static_assert(!COMP || sizeof(T) == 4, "compensated stress: FP32");
@@ -215,7 +215,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   {
     Q4<T> exx = splat4<T>(0), ezz = exx, exz = exx;
     if (act) {
-      tti_rates4<T, BW>(a, s_vx, s_vz, (r + 5) * BW + lx + 4, gi0, gj, true, x.fs, rxx, rzz, rxz);
+      tti_rates4<T, BW, AFDA>(a, s_vx, s_vz, (r + 5) * BW + lx + 4, gi0, gj, true, rxx, rzz, rxz);
       tti_effective4<T, NSLS>(tau, mxx, mzz, mxz, rxx, rzz, rxz, exx, ezz, exz);
     }
     const int e = (r + 1) * EW + lx + 4;
@@ -227,7 +227,7 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
     Q4<T> exx = splat4<T>(0), ezz = exx, exz = exx;
     if (ract) {
       Q4<T> qxx, qzz, qxz;
-      tti_rates4<T, BW>(a, s_vx, s_vz, (rr + 4) * BW + rc, rgi0, rgj, false, x.fs, qxx, qzz, qxz);
+      tti_rates4<T, BW, AFDA>(a, s_vx, s_vz, (rr + 4) * BW + rc, rgi0, rgj, false, qxx, qzz, qxz);
       tti_effective4<T, NSLS>(rtau, qmxx, qmzz, qmxz, qxx, qzz, qxz, exx, ezz, exz);
     }
     const int e = rr * EW + rc;
@@ -336,27 +336,31 @@ __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, cons
   }
 }
 
-template <typename T, int NSLS, bool HINT, bool COMP>
+template <typename T, int NSLS, bool HINT, bool COMP, bool AFDA>
 __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
     k_split_stress_tti(const __grid_constant__ StepArgs<T> a, const __grid_constant__ FusedExtras<T> x,
                        const __grid_constant__ SplitMaps maps) {
-  split_stress_tti_tile<T, NSLS, HINT, COMP>(a, x, maps, blockIdx.x);
+  split_stress_tti_tile<T, NSLS, HINT, COMP, AFDA>(a, x, maps, blockIdx.x);
 }
 
 // Batched: one tile of one shot per CTA; the step parity selects the
 // shot's M / psi buffers.
-template <typename T, int NSLS, bool COMP>
+template <typename T, int NSLS, bool COMP, bool AFDA>
 __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
     k_split_stress_tti_batch(const BatchDev<T> b, int it) {
   int shot, tile;
   batch_locate(b, blockIdx.x, shot, tile);
   FusedExtras<T> x = b.ext[shot];
   x.it = it;
-  // COMP: compensated FP32 shots carry the stress residues, as the unbatched split step
-  split_stress_tti_tile<T, NSLS, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  // COMP: compensated FP32 shots carry the stress residues, as the unbatched
+  // split step; AFDA: some shot has the H-AFDA surface
+  if (AFDA && x.fs == kFsAfda)
+    split_stress_tti_tile<T, NSLS, false, COMP, true>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+  else
+    split_stress_tti_tile<T, NSLS, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
-template <typename T, int NSLS, bool HINT, bool COMP = false>
+template <typename T, int NSLS, bool HINT, bool COMP = false, bool AFDA = false>
 static int launch_tti_k(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
                         cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
@@ -364,12 +368,12 @@ static int launch_tti_k(const StepArgs<T> &a, const FusedExtras<T> &x, const Spl
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti<T, NSLS, HINT, COMP>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti<T, NSLS, HINT, COMP, AFDA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "split TTI stress smem attribute");
     attr_set |= 1ULL << dev;
   }
-  return cuda_check(launch_pdl(k_split_stress_tti<T, NSLS, HINT, COMP>, dim3(ntiles), dim3(G::NT),
+  return cuda_check(launch_pdl(k_split_stress_tti<T, NSLS, HINT, COMP, AFDA>, dim3(ntiles), dim3(G::NT),
                                (size_t)G::SMEM, st, pdl, a, x, m),
                     "split TTI stress launch");
 }
@@ -379,10 +383,17 @@ template <typename T, int NSLS>
 static int launch_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const SplitMaps &m, int ntiles,
                       cudaStream_t st, bool pdl) {
   if constexpr (sizeof(T) == 4) {
-    if (a.slo)
+    if (a.slo) {
+      if (x.fs == kFsAfda)
+        return x.l2hint ? launch_tti_k<T, NSLS, true, true, true>(a, x, m, ntiles, st, pdl)
+                        : launch_tti_k<T, NSLS, false, true, true>(a, x, m, ntiles, st, pdl);
       return x.l2hint ? launch_tti_k<T, NSLS, true, true>(a, x, m, ntiles, st, pdl)
                       : launch_tti_k<T, NSLS, false, true>(a, x, m, ntiles, st, pdl);
+    }
   }
+  if (x.fs == kFsAfda)
+    return x.l2hint ? launch_tti_k<T, NSLS, true, false, true>(a, x, m, ntiles, st, pdl)
+                    : launch_tti_k<T, NSLS, false, false, true>(a, x, m, ntiles, st, pdl);
   return x.l2hint ? launch_tti_k<T, NSLS, true>(a, x, m, ntiles, st, pdl)
                   : launch_tti_k<T, NSLS, false>(a, x, m, ntiles, st, pdl);
 }
@@ -401,48 +412,52 @@ int launch_split_stress_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const
   }
 }
 
-template <typename T, int NSLS, bool COMP>
+template <typename T, int NSLS, bool COMP, bool AFDA>
 static int launch_tti_batch_k(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
   using G = SplitTtiGeom<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti_batch<T, NSLS, COMP>,
+    cudaError_t e = cudaFuncSetAttribute(k_split_stress_tti_batch<T, NSLS, COMP, AFDA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     if (e != cudaSuccess) return cuda_check(e, "batched split TTI stress smem attribute");
     attr_set |= 1ULL << dev;
   }
   if (nitems <= 0) return VI_OK;  // attribute set-up only
-  return cuda_check(launch_pdl(k_split_stress_tti_batch<T, NSLS, COMP>, dim3(nitems), dim3(G::NT),
+  return cuda_check(launch_pdl(k_split_stress_tti_batch<T, NSLS, COMP, AFDA>, dim3(nitems), dim3(G::NT),
                                (size_t)G::SMEM, st, pdl, b, it),
                     "batched split TTI stress launch");
 }
 
 template <typename T, int NSLS>
-static int launch_tti_batch(bool comp, const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
+static int launch_tti_batch(bool comp, bool afda, const BatchDev<T> &b, int it, int nitems, cudaStream_t st,
+                            bool pdl) {
   if constexpr (sizeof(T) == 4)
-    if (comp) return launch_tti_batch_k<T, NSLS, true>(b, it, nitems, st, pdl);
-  return launch_tti_batch_k<T, NSLS, false>(b, it, nitems, st, pdl);
+    if (comp)
+      return afda ? launch_tti_batch_k<T, NSLS, true, true>(b, it, nitems, st, pdl)
+                  : launch_tti_batch_k<T, NSLS, true, false>(b, it, nitems, st, pdl);
+  return afda ? launch_tti_batch_k<T, NSLS, false, true>(b, it, nitems, st, pdl)
+              : launch_tti_batch_k<T, NSLS, false, false>(b, it, nitems, st, pdl);
 }
 
 template <typename T>
-int launch_split_stress_tti_batch(int nsls, bool comp, const BatchDev<T> &b, int it, int nitems,
+int launch_split_stress_tti_batch(int nsls, bool comp, bool afda, const BatchDev<T> &b, int it, int nitems,
                                   cudaStream_t st, bool pdl) {
   switch (nsls) {
-    case 0: return launch_tti_batch<T, 0>(comp, b, it, nitems, st, pdl);
-    case 1: return launch_tti_batch<T, 1>(comp, b, it, nitems, st, pdl);
-    case 2: return launch_tti_batch<T, 2>(comp, b, it, nitems, st, pdl);
-    case 3: return launch_tti_batch<T, 3>(comp, b, it, nitems, st, pdl);
-    case 4: return launch_tti_batch<T, 4>(comp, b, it, nitems, st, pdl);
-    case 5: return launch_tti_batch<T, 5>(comp, b, it, nitems, st, pdl);
+    case 0: return launch_tti_batch<T, 0>(comp, afda, b, it, nitems, st, pdl);
+    case 1: return launch_tti_batch<T, 1>(comp, afda, b, it, nitems, st, pdl);
+    case 2: return launch_tti_batch<T, 2>(comp, afda, b, it, nitems, st, pdl);
+    case 3: return launch_tti_batch<T, 3>(comp, afda, b, it, nitems, st, pdl);
+    case 4: return launch_tti_batch<T, 4>(comp, afda, b, it, nitems, st, pdl);
+    case 5: return launch_tti_batch<T, 5>(comp, afda, b, it, nitems, st, pdl);
     default: return set_error(VI_ERR_ARG, "nsls must be 0..5");
   }
 }
 
-template int launch_split_stress_tti_batch<float>(int, bool, const BatchDev<float> &, int, int,
+template int launch_split_stress_tti_batch<float>(int, bool, bool, const BatchDev<float> &, int, int,
                                                   cudaStream_t, bool);
-template int launch_split_stress_tti_batch<double>(int, bool, const BatchDev<double> &, int, int,
+template int launch_split_stress_tti_batch<double>(int, bool, bool, const BatchDev<double> &, int, int,
                                                    cudaStream_t, bool);
 template int launch_split_stress_tti<float>(const StepArgs<float> &, const FusedExtras<float> &,
                                             const SplitMaps &, int, cudaStream_t, bool);
