@@ -31,7 +31,8 @@ _lib = None
 
 
 def build() -> Path:
-    srcs = [HERE / "visco_oracle.c", HERE / "oracle_step.inc", HERE / "visco_oracle.h"]
+    srcs = [HERE / "visco_oracle.c", HERE / "oracle_step.inc", HERE / "oracle_adjoint.c",
+            HERE / "visco_oracle.h", HERE / "Makefile"]
     if not LIB.exists() or LIB.stat().st_mtime < max(s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
@@ -56,6 +57,13 @@ def lib():
         h.or_stencil8.restype = None
         h.or_stencil8.argtypes = [C.POINTER(C.c_double)]
         h.or_num_threads.restype = C.c_int
+        h.or_adjoint_step_f64.restype = C.c_int
+        h.or_adjoint_step_f64.argtypes = [C.POINTER(ViConfig), C.POINTER(ViMedium), C.POINTER(OrState)]
+        h.or_gradient_f64.restype = C.c_int
+        h.or_gradient_f64.argtypes = [C.POINTER(ViConfig), C.POINTER(ViMedium), C.c_int, C.POINTER(ViSource),
+                                      C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(ViReceiver),
+                                      C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)]
         h.or_afda_weights.restype = None
         h.or_afda_weights.argtypes = [C.POINTER(C.c_double)]
         _lib = h
@@ -141,6 +149,55 @@ def run(w, nsteps: int | None = None, precision: str = "f64", state: OracleState
     if rc != 0:
         raise RuntimeError(f"oracle failed with status {rc}")
     return traces, state
+
+
+def _medium_struct(w, dt=np.float64):
+    arrays = {k: np.ascontiguousarray(v, dtype=dt) for k, v in w.medium.items()}
+    med = ViMedium()
+    for k, a in arrays.items():
+        setattr(med, k, a.ctypes.data)
+    return med, arrays
+
+
+def adjoint_step(w, state: OracleState) -> OracleState:
+    """Applies the transpose of one FP64 step (no sources) to the adjoint
+    state in place (the dot-product partner of run(w, 1) without sources)."""
+    cfg = make_config(w, "f64")
+    med, keep = _medium_struct(w)
+    st = state.struct()
+    rc = lib().or_adjoint_step_f64(C.byref(cfg), C.byref(med), C.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"oracle adjoint failed with status {rc}")
+    del keep
+    return state
+
+
+def gradient(w, obs: np.ndarray, nt: int | None = None):
+    """(J, grad [8, nz, nx]) of the misfit 1/2 sum (d - obs)^2 of an
+    nt-step FP64 run from rest, by the oracle's discrete adjoint (every
+    forward state kept in memory: small grids only)."""
+    nt = w.nt if nt is None else nt
+    cfg = make_config(w, "f64")
+    med, keep = _medium_struct(w)
+    nsrc = len(w.sources)
+    src = (ViSource * max(nsrc, 1))()
+    for q, (i, j, kind, amp) in enumerate(w.sources):
+        src[q].i, src[q].j, src[q].kind, src[q].amp = i, j, kind, amp
+    wav = np.ascontiguousarray(w.wavelets, dtype=np.float64)
+    nrec = len(w.receivers)
+    rec = (ViReceiver * max(nrec, 1))()
+    for r, (i, j) in enumerate(w.receivers):
+        rec[r].i, rec[r].j = i, j
+    obs = np.ascontiguousarray(obs[:, :, :nt], dtype=np.float64)
+    grad = np.zeros((8, w.nz, w.nx))
+    J = C.c_double()
+    P = C.POINTER(C.c_double)
+    rc = lib().or_gradient_f64(C.byref(cfg), C.byref(med), nsrc, src, wav.ctypes.data_as(P), wav.shape[1], nrec,
+                               rec, obs.ctypes.data_as(P), nt, grad.ctypes.data_as(P), C.byref(J))
+    if rc != 0:
+        raise RuntimeError(f"oracle gradient failed with status {rc}")
+    del keep
+    return J.value, grad
 
 
 def cpml_profile(cfg: ViConfig, axis: int, half: int):

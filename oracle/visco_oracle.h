@@ -59,6 +59,22 @@ void or_stencil8(double *D);
 #define AFDA_N 5
 void or_afda_weights(double w[4][4][AFDA_N]);
 
+/* Discrete adjoint of the FP64 step (oracle_adjoint.c): the transposed
+ * stress half and velocity half of one step on an adjoint state a, with
+ * the medium gradient (8 planes) accumulated when g != NULL (x0 / x1: the
+ * forward states before / after the step); the whole transposed step
+ * without sources (dot-product tests); and the misfit gradient of an
+ * nt-step run (every forward state kept: small grids).  Stress-imaging
+ * surface only. */
+int or_adjoint_stress_f64(const vi_config *cfg, const vi_medium *m, const or_state *x0, const or_state *x1,
+                          or_state *a, double *g);
+int or_adjoint_velocity_f64(const vi_config *cfg, const vi_medium *m, const or_state *x0, or_state *a, double *g,
+                            int nsrc, const vi_source *src, const double *wavelet, int wavelet_nt, int it);
+int or_adjoint_step_f64(const vi_config *cfg, const vi_medium *m, or_state *a);
+int or_gradient_f64(const vi_config *cfg, const vi_medium *m, int nsrc, const vi_source *src,
+                    const double *wavelet, int wavelet_nt, int nrec, const vi_receiver *rec, const double *obs,
+                    int nt, double *grad, double *misfit);
+
 /* Number of OpenMP threads the oracle uses. */
 int or_num_threads(void);
 
