@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "fused.cuh"
+#include "nvtx.cuh"
 #include "fused_tma.cuh"
 #include "pdl.cuh"
 #include "plain.cuh"
@@ -1076,12 +1077,15 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   // every segment slot starts at zero: cells the kernels never write (outside
   // the update region, off the CPML strips) stay zero in all of them
   if ((rc = cuda_check(cudaMemsetAsync(seg, 0, (size_t)(K + 1) * sbytes, st), "zero segment"))) return rc;
-  for (int it = 0; it < nt; ++it) {
-    if (it % K == 0)
-      if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, seg, sbytes, cudaMemcpyDeviceToDevice, st),
-                           "checkpoint")))
-        return rc;
-    if ((rc = fwd_step(cur, it, tr, it % K != 0))) return rc;
+  {
+    NvtxRange nr("vi_gradient: forward sweep");
+    for (int it = 0; it < nt; ++it) {
+      if (it % K == 0)
+        if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, seg, sbytes, cudaMemcpyDeviceToDevice, st),
+                             "checkpoint")))
+          return rc;
+      if ((rc = fwd_step(cur, it, tr, it % K != 0))) return rc;
+    }
   }
   if (shot->traces_dev && shot->traces_nt >= nt) {
     for (int k = 0; k < 2 * nrec; ++k)
@@ -1136,6 +1140,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     if ((rc = cuda_check(cudaMemcpyAsync(seg, ck + (size_t)qseg * slot, sbytes, cudaMemcpyDeviceToDevice, st),
                          "restore checkpoint")))
       return rc;
+    NvtxRange nr_seg("vi_gradient: segment recompute and adjoint");
     for (int k = 0; k < s1 - s0; ++k) {
       T *nxt = seg + (size_t)(k + 1) * slot;
       if (use_split) {

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "fused_tma.cuh"
+#include "nvtx.cuh"
 #include "plan.cuh"
 #include "split.cuh"
 
@@ -572,6 +573,7 @@ extern "C" int vi_batch_set_shot(vi_batch *b, int32_t i, const vi_medium *med_de
 
 extern "C" int vi_batch_run(vi_batch *b, int32_t flags, void *stream) {
   if (!b) return set_error(VI_ERR_ARG, "batch is NULL");
+  NvtxRange nr("vi_batch_run");
   cudaStream_t st = (cudaStream_t)stream;
   return b->precision == VI_F64 ? run_impl<double>(b, flags, st) : run_impl<float>(b, flags, st);
 }

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "fused.cuh"
+#include "nvtx.cuh"
 #include "plain.cuh"
 #include "plan.cuh"
 #include "split.cuh"
@@ -598,6 +599,7 @@ extern "C" int vi_plan_workspace_bytes(const vi_plan *p, int64_t *bytes) {
 extern "C" int vi_step(vi_plan *p, const vi_medium *med, vi_fields *f, const vi_shot *shot,
                        int32_t it0, int32_t nsteps, int32_t variant, void *stream) {
   if (!p) return set_error(VI_ERR_ARG, "plan is NULL");
+  NvtxRange nr("vi_step");
   cudaStream_t st = (cudaStream_t)stream;
   return p->cfg.precision == VI_F64
              ? step_impl<double>(p, med, f, shot, it0, nsteps, variant, st)

@@ -36,6 +36,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "nvtx.cuh"
 #include "plan.cuh"
 
 using Clock = std::chrono::steady_clock;
@@ -252,6 +253,7 @@ void release(vi_server *s, Req &q) {
 // Runs the request's next slice (forward) or all of it (gradient); returns
 // true when the request is finished.
 int advance(vi_server *s, Req &q, bool *finished) {
+  NvtxRange nr(q.rq.kind == VI_REQ_GRADIENT ? "vi_serve: gradient request" : "vi_serve: forward slice");
   const vi_request &r = q.rq;
   const size_t es = esize_of(r.cfg);
   int rc;
