@@ -86,6 +86,10 @@ static void set_order(vi_batch *b) {
 // Builds every per-shot device structure for one kernel form and uploads it.
 template <typename T>
 static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
+  // one tile list serves both merged split kernels: their tilings must agree
+  static_assert(SplitGeom<T>::TX == SplitStressGeomBatch<T>::TX && SplitGeom<T>::TZ == SplitStressGeomBatch<T>::TZ &&
+                    SplitGeom<T>::TX == SplitTtiGeomBatch<T>::TX && SplitGeom<T>::TZ == SplitTtiGeomBatch<T>::TZ,
+                "merged split kernels share one tiling");
   const bool split = form == kFormSplit;
   const bool tti = b->kind == VI_MEDIUM_TTI;
   TmaBoxes bx{};
@@ -163,8 +167,8 @@ static int prepare(vi_batch *b, int form, cudaStream_t st, BatchDev<T> &bd) {
         s.psiz_o = psiz0 ? psiz0 + pout * kPsiPerSet * p->psiz_plane : nullptr;
         args[2 * i + par] = s;
       }
-      const int bw = tti ? SplitTtiGeom<T>::BW : SplitStressGeom<T>::BW;
-      const int bh = tti ? SplitTtiGeom<T>::BH : SplitStressGeom<T>::BH;
+      const int bw = tti ? SplitTtiGeomBatch<T>::BW : SplitStressGeomBatch<T>::BW;
+      const int bh = tti ? SplitTtiGeomBatch<T>::BH : SplitStressGeomBatch<T>::BH;
       if ((rc = encode_map(&smaps[i].a, a.vx, (int)sizeof(T), c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
       if ((rc = encode_map(&smaps[i].b, a.vz, (int)sizeof(T), c.nx, c.nz, 1, 0, bw, bh, 1))) return rc;
       smaps[i].c = smaps[i].b;

@@ -291,6 +291,7 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
       zzz = fma4(splat4<T>(cq), v, zzz);
     }
   }
+  static_assert(G::TZ >= 4, "the H-AFDA rows below the surface lie in the first tile row");
   if (AFDA && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L)
     const int qs = gj - L;
     zxz = afda4<0>(a, qs, [&](int m) { return lds4(s_sxz + (m + 4) * WX + lx + 4); });
@@ -340,11 +341,11 @@ __global__ void __launch_bounds__(SplitGeom<T>::NT, (sizeof(T) == 4 ? 1024 : 512
 // output one (a.sxx_o.., a.m_o, a.psix_o/psiz_o; the v maps then cover the
 // output velocities); else in place.  COMP (FP32, in place): sigma is
 // accumulated with its rounding residue (a.slo, two_sum_acc4).
-template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false, bool AFDA = false>
+template <typename T, int KIND, int NSLS, bool OOP, bool HINT, bool COMP = false, bool AFDA = false,
+          typename G = SplitStressGeom<T>>
 __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                   const SplitMaps &maps, int tile) {
   static_assert(!COMP || (sizeof(T) == 4 && !OOP), "compensated stress: FP32, in place");
-  using G = SplitStressGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, SW = G::BW, PB = G::PB;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
@@ -425,10 +426,11 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
       zvx = fma4(splat4<T>(cq), v, zvx);
     }
   }
-  if (AFDA && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (z0 == L;
-    const int qs = gj - L;              // on the surface row the tau_zz = 0 relation sets e_zz)
-    if (qs >= 1) zvz = afda4<2>(a, qs, [&](int m) { return lds4(s_vz + (m + 4) * SW + lx + 4); });
-    if (qs < 3) zvx = afda4<3>(a, qs, [&](int m) { return lds4(s_vx + (m + 4) * SW + lx + 4); });
+  if (AFDA && gj < L + 4) {  // one-sided z derivatives below the H-AFDA surface (grid row L + m
+    const int qs = gj - L;     // is box row L + m - (z0 - 4); on the surface row the tau_zz = 0
+    const int b0 = L + 4 - z0; // relation sets e_zz)
+    if (qs >= 1) zvz = afda4<2>(a, qs, [&](int m) { return lds4(s_vz + (m + b0) * SW + lx + 4); });
+    if (qs < 3) zvx = afda4<3>(a, qs, [&](int m) { return lds4(s_vx + (m + b0) * SW + lx + 4); });
   }
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 
 }
 
 template <typename T, int KIND, int NSLS, bool COMP, bool AFDA>
-__global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeom<T>::NT)
+__global__ void __launch_bounds__(SplitStressGeomBatch<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitStressGeomBatch<T>::NT)
     k_split_stress_batch(const BatchDev<T> b, int it) {
   int shot, tile;
   batch_locate(b, blockIdx.x, shot, tile);
@@ -575,10 +577,13 @@ __global__ void __launch_bounds__(SplitStressGeom<T>::NT, (sizeof(T) == 4 ? 512 
   x.it = it;
   // COMP: compensated FP32 shots carry the stress residues, as the unbatched
   // split step; AFDA: some shot has the H-AFDA surface
+  using G = SplitStressGeomBatch<T>;
   if (AFDA && x.fs == kFsAfda)
-    split_stress_tile<T, KIND, NSLS, false, false, COMP, true>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+    split_stress_tile<T, KIND, NSLS, false, false, COMP, true, G>(b.args[2 * shot + (it & 1)], x, b.smaps[shot],
+                                                                  tile);
   else
-    split_stress_tile<T, KIND, NSLS, false, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+    split_stress_tile<T, KIND, NSLS, false, false, COMP, false, G>(b.args[2 * shot + (it & 1)], x, b.smaps[shot],
+                                                                   tile);
 }
 
 // ------------------------------------------------------------------- host
@@ -672,7 +677,7 @@ int launch_split_vel_batch(int kind, bool afda, const BatchDev<T> &b, int it, in
 
 template <typename T, int KIND, int NSLS, bool COMP, bool AFDA>
 static int launch_stress_batch_k(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
-  using SG = SplitStressGeom<T>;
+  using SG = SplitStressGeomBatch<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);

@@ -23,12 +23,15 @@ struct SplitGeom {
   static constexpr int SMEM_STRESS = 128 + 2 * PB * (int)sizeof(T);
 };
 
-// Tiling of the stress kernel: 64 x STRESS_TZ cells, one 4-cell group per
-// thread, the new velocities staged as a TMA box with a 4-cell halo.
-constexpr int kStressTZ = 8;
-template <typename T>
-struct SplitStressGeom {
-  static constexpr int TX = 64, TZ = kStressTZ, NT = TX / 4 * TZ;
+// Tiling of the stress kernel: TX_ x TZ_ cells, one 4-cell group per
+// thread, the new velocities staged as a TMA box with a 4-cell halo.  The
+// single-shot step uses 128 x 2 tiles (their rows are 512-byte runs of each
+// of the ~30 planes the pass streams: 54.5 vs 55.9 us per 2048 x 1024 VTI
+// step for 64 x 8, 54.8 for 128 x 4, 58.2 for 128 x 8); the merged batch
+// kernels keep 64 x 8, the tiling of their shared tile lists.
+template <typename T, int TX_, int TZ_>
+struct SplitStressGeomT {
+  static constexpr int TX = TX_, TZ = TZ_, NT = TX / 4 * TZ;
   static constexpr int BW = TX + 8, BH = TZ + 8;
   static constexpr int PB =
       (int)(((long long)BW * BH * (long long)sizeof(T) + 127) / 128 * 128 / (long long)sizeof(T));
@@ -36,13 +39,19 @@ struct SplitStressGeom {
   static constexpr int BOX_BYTES = BW * BH * (int)sizeof(T);
   static constexpr int SMEM = 128 + 2 * PB * (int)sizeof(T);
 };
+template <typename T>
+using SplitStressGeom = SplitStressGeomT<T, 128, 2>;
+template <typename T>
+using SplitStressGeomBatch = SplitStressGeomT<T, 64, 8>;
 
-// Tiling of the TTI stress kernel: 64 x 8 cells; the effective rates are
+// Tiling of the TTI stress kernel: TX_ x TZ_ cells; the effective rates are
 // computed on the tile and a one-cell ring (4-aligned: EW x EH), from a TMA
 // box of the new velocities with the ring's 4-cell stencil halo (BW x BH).
-template <typename T>
-struct SplitTtiGeom {
-  static constexpr int TX = 64, TZ = 8, NT = TX / 4 * TZ;
+// Single shot 128 x 4 (73.8 vs 75.6 us per 2048 x 1024 TTI step for
+// 64 x 8); the merged batch kernels keep 64 x 8.
+template <typename T, int TX_, int TZ_>
+struct SplitTtiGeomT {
+  static constexpr int TX = TX_, TZ = TZ_, NT = TX / 4 * TZ;
   static constexpr int BW = TX + 16, BH = TZ + 10;
   static constexpr int EW = TX + 8, EH = TZ + 2;
   static constexpr int PB =
@@ -55,6 +64,10 @@ struct SplitTtiGeom {
   static constexpr int NRING = 2 * (EW / 4) + 2 * TZ;  // ring groups: 2 rows + 2 columns
   static_assert(NRING <= NT, "one ring group per thread at most");
 };
+template <typename T>
+using SplitTtiGeom = SplitTtiGeomT<T, 128, 4>;
+template <typename T>
+using SplitTtiGeomBatch = SplitTtiGeomT<T, 64, 8>;
 
 // TMA maps of the staged planes: (sxx, szz, sxz) for the velocity kernel,
 // (vx, vz) for the stress kernel.

@@ -152,11 +152,10 @@ __device__ __forceinline__ Q4<T> mean4_fwd(const Q4<T> &a, T a4, const Q4<T> &b,
 }
 
 // COMP (FP32): sigma accumulated with its rounding residue (a.slo, two_sum_acc4).
-template <typename T, int NSLS, bool HINT, bool COMP = false, bool AFDA = false>
+template <typename T, int NSLS, bool HINT, bool COMP = false, bool AFDA = false, typename G = SplitTtiGeom<T>>
 __device__ __forceinline__ void split_stress_tti_tile(const StepArgs<T> &a, const FusedExtras<T> &x,
                                                       const SplitMaps &maps, int tile) {
   static_assert(!COMP || sizeof(T) == 4, "compensated stress: FP32");
-  using G = SplitTtiGeom<T>;
   constexpr int TX = G::TX, TZ = G::TZ, BW = G::BW, EW = G::EW, EG = G::EW / 4;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
@@ -346,7 +345,7 @@ __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 2
 // Batched: one tile of one shot per CTA; the step parity selects the
 // shot's M / psi buffers.
 template <typename T, int NSLS, bool COMP, bool AFDA>
-__global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeom<T>::NT)
+__global__ void __launch_bounds__(SplitTtiGeomBatch<T>::NT, (sizeof(T) == 4 ? 512 : 256) / SplitTtiGeomBatch<T>::NT)
     k_split_stress_tti_batch(const BatchDev<T> b, int it) {
   int shot, tile;
   batch_locate(b, blockIdx.x, shot, tile);
@@ -354,10 +353,11 @@ __global__ void __launch_bounds__(SplitTtiGeom<T>::NT, (sizeof(T) == 4 ? 512 : 2
   x.it = it;
   // COMP: compensated FP32 shots carry the stress residues, as the unbatched
   // split step; AFDA: some shot has the H-AFDA surface
+  using G = SplitTtiGeomBatch<T>;
   if (AFDA && x.fs == kFsAfda)
-    split_stress_tti_tile<T, NSLS, false, COMP, true>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+    split_stress_tti_tile<T, NSLS, false, COMP, true, G>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
   else
-    split_stress_tti_tile<T, NSLS, false, COMP>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
+    split_stress_tti_tile<T, NSLS, false, COMP, false, G>(b.args[2 * shot + (it & 1)], x, b.smaps[shot], tile);
 }
 
 template <typename T, int NSLS, bool HINT, bool COMP = false, bool AFDA = false>
@@ -414,7 +414,7 @@ int launch_split_stress_tti(const StepArgs<T> &a, const FusedExtras<T> &x, const
 
 template <typename T, int NSLS, bool COMP, bool AFDA>
 static int launch_tti_batch_k(const BatchDev<T> &b, int it, int nitems, cudaStream_t st, bool pdl) {
-  using G = SplitTtiGeom<T>;
+  using G = SplitTtiGeomBatch<T>;
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device set up (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
