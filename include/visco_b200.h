@@ -196,14 +196,27 @@ int vi_plan_last_kernel(const vi_plan *plan, int32_t *kernel);
  * 7 = streaming kernel (FP32 ISO/VTI: persistent CTAs march down 128-column
  * strips with TMA row rings, one launch per step),
  * 8 = the split pair of 5 with its velocity pass reading the stress taps
- * straight through L1 instead of TMA boxes.
- * Variants 3-8 return VI_ERR_ARG when not eligible.
+ * straight through L1 instead of TMA boxes, 9 = the split pair's tiles
+ * time-blocked: one persistent kernel per call runs sweeps of several
+ * steps as a wavefront over 8-row bands, so the next steps re-read a
+ * band's state from L2 (ISO/VTI, imaging or no free surface, not
+ * VI_F32C; depth and lag set by vi_plan_set_wave; results bitwise equal
+ * to variant 5).
+ * Variants 3-9 return VI_ERR_ARG when not eligible.
  * VI_F32C plans (split pair only) keep the stresses' rounding residues as
  * plan state, continued across calls like the CPML memory: vi_plan_reset
  * zeroes them. */
 int vi_step(vi_plan *plan, const vi_medium *med_dev, vi_fields *fields_dev,
             const vi_shot *shot, int32_t it0, int32_t nsteps,
             int32_t kernel_variant, void *stream);
+
+/* Time blocking of kernel variant 9: sweeps of `depth` steps (0 = the
+ * default, 4) with a lag of `lag` 8-row bands between consecutive passes
+ * (0 = the default, 8; else 2 .. 64).  Deeper sweeps re-read more steps'
+ * state from L2; a longer lag lets a pass's units find their inputs done
+ * but keeps more bands in flight.  No counterpart in the reference, which
+ * runs one launch per step (visco-kernels.jl:87-100). */
+int vi_plan_set_wave(vi_plan *plan, int32_t depth, int32_t lag);
 
 /* Same steps as vi_step with kernel_variant 1 (plain, in place), but it
  * allocates no device memory: its strain planes and source/receiver lists

@@ -130,6 +130,7 @@ _SIGNATURES = [
     ("vi_plan_workspace_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("vi_plan_status", C.c_int, [C.c_void_p, C.c_void_p]),
     ("vi_plan_last_kernel", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("vi_plan_set_wave", C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     ("vi_step", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.POINTER(ViFields),
                           C.POINTER(ViShot), C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     ("vi_step_noalloc", C.c_int, [C.c_void_p, C.POINTER(ViMedium), C.POINTER(ViFields),

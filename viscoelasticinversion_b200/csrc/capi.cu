@@ -378,7 +378,7 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
   rc = check_fields(p, f);
   if (rc) return rc;
   if (nsteps < 0) return set_error(VI_ERR_ARG, "nsteps must be >= 0");
-  if (variant < 0 || variant > 8) return set_error(VI_ERR_ARG, "unknown kernel variant");
+  if (variant < 0 || variant > 9) return set_error(VI_ERR_ARG, "unknown kernel variant");
   if (s && s->nrec > 0 && s->traces_nt > 0 && !s->traces_dev)
     return set_error(VI_ERR_ARG, "receivers need traces_dev");
   rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice");
@@ -432,6 +432,10 @@ static int step_impl(vi_plan *p, const vi_medium *m, vi_fields *f, const vi_shot
     } else {
       return set_error(VI_ERR_ARG, "the streaming step is FP32 only");
     }
+  } else if (variant == 9) {
+    rc = wave_steps<T>(p, a, s, it0, nsteps, st);
+    if (rc) return rc;
+    p->last_kernel = 9;
   } else if (p->cfg.precision == VI_F32C &&
              !(variant == 5 || variant == 8 || (variant == 0 && split_eligible<T>(p, a)))) {
     return set_error(VI_ERR_ARG, "compensated FP32 (VI_F32C) runs on the split pair only (kernel variant 0, 5 or 8 "
@@ -538,13 +542,22 @@ fail:
   return rc;
 }
 
+extern "C" int vi_plan_set_wave(vi_plan *p, int32_t depth, int32_t lag) {
+  if (!p) return set_error(VI_ERR_ARG, "null plan");
+  if (depth < 0 || depth > 64) return set_error(VI_ERR_ARG, "wavefront depth must be 0 (default) .. 64 steps");
+  if (lag != 0 && (lag < 2 || lag > 64)) return set_error(VI_ERR_ARG, "wavefront band lag must be 0 (default) or 2 .. 64");
+  p->wave_k = depth;
+  p->wave_d = lag;
+  return VI_OK;
+}
+
 extern "C" int vi_plan_destroy(vi_plan *p) {
   if (!p) return VI_OK;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(p->device);
   void *bufs[] = {p->psix, p->psiz, p->tabx, p->tabz, p->scratch, p->alt, p->slo,
-                  p->dsrc, p->damp, p->drec, p->tile_lists, p->fwd, p->errflag};
+                  p->dsrc, p->damp, p->drec, p->tile_lists, p->fwd, p->errflag, p->wave_ctl};
   for (void *b : bufs)
     if (b) cudaFree(b);
   cudaSetDevice(prev);

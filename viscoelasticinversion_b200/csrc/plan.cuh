@@ -34,6 +34,11 @@ struct vi_plan {
   // fused path: per-tile source / receiver lists (device, grown on demand)
   void *tile_lists = nullptr;
   size_t tile_lists_bytes = 0;
+  // wavefront step: ticket, abort flag and per-band completion counters;
+  // sweep depth (steps) and band lag, 0 = the built-in defaults
+  void *wave_ctl = nullptr;
+  size_t wave_ctl_bytes = 0;
+  int wave_k = 0, wave_d = 0;
   // forward_host buffers (device, grown on demand)
   void *fwd = nullptr;
   size_t fwd_bytes = 0;

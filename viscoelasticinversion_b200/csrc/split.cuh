@@ -131,6 +131,16 @@ template <typename T>
 int split_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st,
                 int mode);
 
+// The time-blocked form of the split pair (wave.cu): one persistent
+// kernel runs sweeps of k steps as a wavefront over 8-row bands, with a
+// lag of d bands between consecutive passes (plan's wave_k / wave_d, 0 =
+// these defaults).  ISO/VTI, imaging or no free surface, FP32 or FP64 (not
+// VI_F32C); same eligibility as split_steps otherwise.
+constexpr int kWaveDefaultK = 4, kWaveDefaultD = 8;
+bool wave_eligible_cfg(const vi_config &c);
+template <typename T>
+int wave_steps(vi_plan *p, StepArgs<T> a, const vi_shot *s, int it0, int nsteps, cudaStream_t st);
+
 // true when split_steps can run this plan and these pointers
 template <typename T>
 bool split_eligible(const vi_plan *p, const StepArgs<T> &a);

@@ -36,6 +36,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Ends the barrier's use, so its word may be initialised again (a CTA
+// that runs many tiles re-arms one barrier per tile).
+__device__ __forceinline__ void mbar_inval(uint64_t *bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Orders this thread's earlier generic-proxy accesses (and those made
+// visible to it) before its later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async;" ::: "memory");
+}
+
 // Bounded wait: gives up after max_tries polls (each poll may suspend the
 // thread for a hardware-defined interval) and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,

@@ -98,6 +98,31 @@ __device__ __forceinline__ Q4<double> ldh4(const double *p, uint64_t pol) {
   asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[2]), "=d"(q.v[3]) : "l"(p + 2), "l"(pol));
   return q;
 }
+// State loaded before the PDL wait (written by the grid before the running
+// one, which completed before this grid was released): read at L2, the
+// coherence point, never from a line an earlier grid left in this SM's L1.
+__device__ __forceinline__ Q4<float> ldcgh4(const float *p, uint64_t pol) {
+  Q4<float> q;
+  asm volatile("ld.global.cg.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(q.v[0]), "=f"(q.v[1]), "=f"(q.v[2]), "=f"(q.v[3])
+               : "l"(p), "l"(pol));
+  return q;
+}
+__device__ __forceinline__ Q4<double> ldcgh4(const double *p, uint64_t pol) {
+  Q4<double> q;
+  asm volatile("ld.global.cg.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[0]), "=d"(q.v[1]) : "l"(p), "l"(pol));
+  asm volatile("ld.global.cg.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(q.v[2]), "=d"(q.v[3]) : "l"(p + 2), "l"(pol));
+  return q;
+}
+__device__ __forceinline__ Q4<float> ldcg4(const float *p) {
+  const float4 q = __ldcg(reinterpret_cast<const float4 *>(p));
+  return {{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ Q4<double> ldcg4(const double *p) {
+  const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+  return {{a.x, a.y, b.x, b.y}};
+}
 __device__ __forceinline__ Q4<float> ldgh4(const float *p, uint64_t pol) {  // read-only data
   Q4<float> q;
   asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"

@@ -88,6 +88,10 @@ def _stream_handle(stream) -> int | None:
     return getattr(stream, "cuda_stream", stream)
 
 
+# tune() choices per grid class: (nx, nz, medium, nsls, precision, free surface)
+_TUNED: dict = {}
+
+
 class StepPlan:
     """Owns one vi_plan: CPML profiles and ψ memory, the fused path's second
     state copy and the staged source/receiver lists."""
@@ -144,7 +148,7 @@ class StepPlan:
         k = C.c_int32()
         check(lib().vi_plan_last_kernel(self._h, C.byref(k)))
         return {0: "none", 1: "plain", 2: "fused", 3: "fused-tma", 4: "fused-tma-1stage",
-                5: "split", 6: "split-pipelined", 7: "stream", 8: "split-ldg"}[k.value]
+                5: "split", 6: "split-pipelined", 7: "stream", 8: "split-ldg", 9: "wave"}[k.value]
 
     def zeros_state(self) -> dict:
         """Zeroed device state {vx, vz, sxx, szz, sxz, m}."""
@@ -211,9 +215,70 @@ class StepPlan:
         return shot, keep
 
     # ---- stepping ----------------------------------------------------------
+    # (depth, lag) of the time-blocked step tried by tune()
+    WAVE_CANDIDATES = ((2, 4), (4, 4), (4, 8), (8, 8), (16, 8))
+
+    def tune(self, medium: dict, nsteps: int = 32, reps: int = 2, candidates=None) -> dict:
+        """Autotuner of the step's kernel form for this grid class: times
+        the split pair (kernel variant 5) and the time-blocked step (variant
+        9) at each (depth, lag) on a scratch state of this plan with the
+        caller's medium, keeps the fastest, and makes it the choice of
+        step(..., variant="auto") for every plan of the same class (grid,
+        medium kind, N_sls, precision, free surface).  Returns
+        {"variant", "depth", "lag", "us_per_step": {form: us}}."""
+        key = self._tune_key()
+        st = self.zeros_state()
+        table = {}
+        forms = [(5, 0, 0)]
+        if self.cfg.medium != _abi.VI_MEDIUM_TTI and self.cfg.precision != _abi.VI_F32C and \
+                self.cfg.free_surface != FREE_SURFACE_HAFDA and self.nx % 4 == 0:
+            forms += [(9, k, d) for k, d in (candidates or self.WAVE_CANDIDATES)]
+        best = None
+        for variant, k, d in forms:
+            if variant == 9:
+                self.set_wave(k, d)
+            self.step(medium, st, nsteps=nsteps, variant=variant)  # warm-up
+            ms = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                self.step(medium, st, nsteps=nsteps, variant=variant)
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            us = min(ms) * 1e3 / nsteps
+            name = "split" if variant == 5 else f"wave k={k} d={d}"
+            table[name] = us
+            if best is None or us < best[0]:
+                best = (us, variant, k, d)
+        del st
+        self.reset()
+        _, variant, k, d = best
+        self.set_wave(k, d)
+        choice = {"variant": variant, "depth": k, "lag": d, "us_per_step": table}
+        _TUNED[key] = choice
+        return choice
+
+    def _tune_key(self):
+        c = self.cfg
+        return (c.nx, c.nz, c.medium, c.nsls, c.precision, c.free_surface)
+
+    def set_wave(self, depth: int = 0, lag: int = 0):
+        """Time blocking of kernel variant 9: sweeps of `depth` steps with
+        `lag` bands between consecutive passes (0 = the built-in defaults)."""
+        check(lib().vi_plan_set_wave(self._h, int(depth), int(lag)))
+
     def step(self, medium: dict, state: dict, nsteps: int = 1, it0: int = 0, sources=None,
-             wavelets=None, receivers=None, traces=None, variant: int = 0, stream=None):
-        """Advances state {v, s, m} by nsteps in place (asynchronous on stream)."""
+             wavelets=None, receivers=None, traces=None, variant=0, stream=None):
+        """Advances state {v, s, m} by nsteps in place (asynchronous on stream).
+        variant="auto": the form tune() chose for this grid class (tuned
+        on first use)."""
+        if variant == "auto":
+            choice = _TUNED.get(self._tune_key())
+            if choice is None:
+                choice = self.tune(medium)
+            self.set_wave(choice["depth"], choice["lag"])
+            variant = choice["variant"]
         v, s, m = state["v"], state["s"], state.get("m")
         f = self.fields_struct(v[0], v[1], s[0], s[1], s[2], m if self.nsls else None)
         med = self._medium_struct(medium)
