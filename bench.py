@@ -58,7 +58,11 @@ def parse_args():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-grad", action="store_true")
     p.add_argument("--grad-nt", type=int, default=3000)
+    p.add_argument("--grad-shots", type=int, default=16)
     p.add_argument("--serve-requests", type=int, default=40)
+    p.add_argument("--serve-full", action="store_true",
+                   help="the request stream as specified (every grid for both kinds, nt 1000..8000); "
+                        "use with --serve-requests of a few hundred")
     p.add_argument("--serve-explore", action="store_true",
                    help="time several slice lengths and both scheduling policies")
     return p.parse_args()
@@ -307,10 +311,14 @@ def measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=False):
 
 
 def measure_serving(a, dev, seed=0):
-    """Request serving on a bounded sample of the mixed request stream:
-    Poisson arrivals at 50 requests/s, 70 % forward / 30 % gradient, grids
-    from {256², 1024x512, 2048x1024, 4096x2048}, media from {iso, VTI, TTI}
-    (gradients: iso/VTI), step counts a quarter of [1000, 8000].  The same
+    """Request serving on the mixed request stream: Poisson arrivals at 50
+    requests/s, 70 % forward / 30 % gradient, media from {iso, VTI, TTI}.
+    Default (bounded sample, a.serve_requests requests): forward grids from
+    {256², 1024x512, 2048x1024, 4096x2048} (4096x2048 as iso/VTI: its tilt
+    field takes ~15 s to generate), gradient grids from {256², 1024x512},
+    step counts a quarter of [1000, 8000].  a.serve_full: the stream as
+    specified for both kinds (every grid, every medium, nt in [1000,
+    8000]).  The same
     arrivals are served twice: by the server with time slices given to the
     request with the least remaining work (continuous batching) and FIFO one
     request at a time with no slicing (one lane).  Slices are 1024 steps;
@@ -331,7 +339,7 @@ def measure_serving(a, dev, seed=0):
 
     def workload(g, kind):
         if (g, kind) not in base:
-            base[(g, kind)] = media.layered(nx=g[0], nz=g[1], nt=2000, kind=kind, seed=7,
+            base[(g, kind)] = media.layered(nx=g[0], nz=g[1], nt=8000 if a.serve_full else 2000, kind=kind, seed=7,
                                             pml=20 if g[0] <= 256 else 40, nrec=64,
                                             nlayers=4)
         return base[(g, kind)]
@@ -341,11 +349,11 @@ def measure_serving(a, dev, seed=0):
     for _ in range(n):
         t += rng.exponential(1 / 50.0)
         grad = rng.random() < 0.3
-        kind = ("iso", "vti")[rng.integers(2)] if grad else ("iso", "vti", "tti")[rng.integers(3)]
-        g = grids[rng.integers(2)] if grad else grids[rng.integers(len(grids))]
-        if g == (4096, 2048) and kind == "tti":
+        kind = ("iso", "vti", "tti")[rng.integers(3)]
+        g = grids[rng.integers(2)] if grad and not a.serve_full else grids[rng.integers(len(grids))]
+        if g == (4096, 2048) and kind == "tti" and not a.serve_full:
             kind = "vti"  # the tilt field of a 4096x2048 TTI medium takes ~15 s to generate
-        nt = int(rng.integers(250, 2001))
+        nt = int(rng.integers(1000, 8001)) if a.serve_full else int(rng.integers(250, 2001))
         w0 = workload(g, kind)
         w = dataclasses.replace(w0, nt=nt, wavelets=w0.wavelets[:, :nt])
         reqs.append((t, grad, w))
@@ -382,14 +390,17 @@ def measure_serving(a, dev, seed=0):
     for (g, kind), w0 in base.items():
         w = dataclasses.replace(w0, nt=8, wavelets=w0.wavelets[:, :8])
         warm.append(srv.submit_forward(w, "f32"))
-        if kind != "tti" and g[0] <= 1024:
+        if g[0] <= 1024:
             warm.append(srv.submit_gradient(w, np.zeros((2, len(w.receivers), 8), np.float32), "f32"))
     for tk in warm:
         srv.wait(tk)
     srv.stop()
     pts = sum(w.nx * w.nz * w.nt * (3 if grad else 1) for _, grad, w in reqs)
-    out = {"workload": f"{n} requests, Poisson 50/s, 70% forward / 30% gradient, grids 256^2..4096x2048, "
-                       "iso/VTI/TTI (4096x2048: iso/VTI), nt 250..2000 (a quarter of 1000..8000), f32",
+    out = {"workload": (f"{n} requests, Poisson 50/s, 70% forward / 30% gradient, grids 256^2..4096x2048, "
+                        "iso/VTI/TTI, nt 1000..8000, f32" if a.serve_full else
+                        f"{n} requests, Poisson 50/s, 70% forward / 30% gradient, grids 256^2..4096x2048 "
+                        "(gradients 256^2 and 1024x512), iso/VTI/TTI (4096x2048 forward: iso/VTI), "
+                        "nt 250..2000 (a quarter of 1000..8000), f32"),
            "forward": sum(1 for _, g, _ in reqs if not g), "gradient": sum(1 for _, g, _ in reqs if g)}
     runs = [("sequential", (1 << 30, 1, "shortest-first", 1))] + [(n_, c) for n_, c in a.serve_policies]
     for name, (sl, ma, pol, ln) in runs:
@@ -400,13 +411,18 @@ def measure_serving(a, dev, seed=0):
     return out
 
 
-def measure_gradient(a, dev):
-    """Misfit gradient of one shot of the 1024 x 512, 3000-step FP32 VTI
-    gradient workload (C2 recipe, start model Gaussian-smoothed with
-    sigma = 100 m, observed traces from the true model), through
-    vi_gradient: seconds, grid-point steps per second of the whole gradient
-    (forward + recompute + adjoint), and the misfit.  A first gradient of
-    the same shot (untimed) sizes the plan's checkpoint workspace."""
+def measure_gradient_c4(a, dev):
+    """The FWI-gradient workload as specified: 16 shots on the 1024 x 512,
+    3000-step VTI model (sources every 1/17 of the width at the workload's
+    source depth, 512 receivers), FP32 wavefields, FP64 accumulation of the
+    summed gradient through vi_gradient (accumulate), start model smoothed
+    100 m, observed data from the true model.  Timed: the 16 gradients.
+    Untimed checks on shot 1: the same gradient with FP64 wavefields
+    (FP64 observed data) and its central differences (h = 1e-3 of the cell
+    value) of the FP64 forward misfit at 20 seeded cells drawn among the
+    top decile of |g| in the interior, over the rho, c11, c13, c33, c55 and
+    tau planes; and the relative L2 error of the FP32 gradient against the
+    FP64 one, per plane."""
     import numpy as np
     import torch
     from scipy.ndimage import gaussian_filter
@@ -414,33 +430,86 @@ def measure_gradient(a, dev):
     from viscoelasticinversion_b200 import StepPlan, media
     from viscoelasticinversion_b200.gradient import misfit_gradient
 
+    nshots = a.grad_shots
     true = media.layered(nx=1024, nz=512, nt=a.grad_nt, kind="vti", seed=3)
-    start = dict(true.medium)
-    for k in start:
-        start[k] = gaussian_filter(true.medium[k], 100.0 / true.dx, mode="nearest")
+    start = {k: gaussian_filter(v, 100.0 / true.dx, mode="nearest") for k, v in true.medium.items()}
+    sj = true.sources[0][1]
+    xs = [int(round((n + 1) * true.nx / (nshots + 1))) for n in range(nshots)]
+    shots = [[(i, sj, 0, 1.0)] for i in xs]
+
+    def observed(plan, wav, srcs):
+        med_t = plan.medium_to_device(true.medium)
+        obs = torch.zeros(2, len(true.receivers), true.nt, dtype=plan.dtype, device=plan.device)
+        st = plan.zeros_state()
+        plan.reset()
+        plan.step(med_t, st, nsteps=true.nt, sources=srcs, wavelets=wav, receivers=true.receivers, traces=obs)
+        plan.status()
+        return obs
+
     plan = StepPlan.for_workload(true, "f32", device=dev.index)
     wav = torch.as_tensor(true.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
-    obs = torch.zeros(2, len(true.receivers), true.nt, dtype=plan.dtype, device=plan.device)
-    med_t = plan.medium_to_device(true.medium)
-    st = plan.zeros_state()
-    plan.reset()
-    plan.step(med_t, st, nsteps=true.nt, sources=true.sources, wavelets=wav,
-              receivers=true.receivers, traces=obs)
-    plan.status()
+    obs = [observed(plan, wav, s) for s in shots]
     med = plan.medium_to_device(start)
-    # warm-up at the full length: the plan's checkpoint workspace is
-    # allocated once and reused by every later gradient of the shot size
-    misfit_gradient(plan, med, true.sources, wav, true.receivers, obs)
+    misfit_gradient(plan, med, shots[0], wav, true.receivers, obs[0])  # sizes the checkpoint workspace
+    g = torch.zeros(8, plan.nz, plan.nx, dtype=torch.float64, device=plan.device)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    J, g = misfit_gradient(plan, med, true.sources, wav, true.receivers, obs)
+    J = 0.0
+    for n in range(nshots):
+        Jn, _ = misfit_gradient(plan, med, shots[n], wav, true.receivers, obs[n], grad=g, accumulate=n > 0)
+        J += Jn
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
+    g1_32 = misfit_gradient(plan, med, shots[0], wav, true.receivers, obs[0])[1].clone()
     plan.close()
-    pts = true.nx * true.nz * true.nt
-    return {"workload": f"vti-1024x512-nt{true.nt}-f32-gradient (start model smoothed 100 m)",
-            "seconds": sec, "gpts": pts / sec / 1e9, "misfit": J,
-            "grad_finite": bool(torch.isfinite(g).all().item())}
+    # FP64 wavefields: gradient of shot 1 and central differences of its misfit
+    p64 = StepPlan.for_workload(true, "f64", device=dev.index)
+    wav64 = torch.as_tensor(true.wavelets, dtype=torch.float64, device=p64.device).contiguous()
+    obs64 = observed(p64, wav64, shots[0])
+    med64 = p64.medium_to_device(start)
+    _, g64 = misfit_gradient(p64, med64, shots[0], wav64, true.receivers, obs64)
+    g64 = g64.clone()
+    tr = torch.zeros_like(obs64)
+
+    def misfit64(m):
+        st = p64.zeros_state()
+        p64.reset()
+        p64.step(m, st, nsteps=true.nt, sources=shots[0], wavelets=wav64, receivers=true.receivers, traces=tr)
+        p64.status()
+        return 0.5 * float(((tr - obs64) ** 2).sum().item())
+
+    planes = {"rho": 0, "c11": 1, "c13": 2, "c33": 4, "c55": 6, "tau": 7}
+    rng = np.random.default_rng(7)
+    pml = true.pml + 8
+    fd = []
+    for n in range(20):
+        name = list(planes)[n % len(planes)]
+        gp = g64[planes[name], pml:-pml, pml:-pml].abs()
+        thr = torch.quantile(gp.flatten()[:: max(1, gp.numel() // 1_000_000)], 0.9).item()
+        cand = torch.nonzero(gp >= thr).cpu().numpy()
+        j, i = cand[rng.integers(len(cand))] + pml
+        base = med64[name][j, i].item()
+        h = 1e-3 * abs(base)
+        med64[name][j, i] = base + h
+        jp = misfit64(med64)
+        med64[name][j, i] = base - h
+        jm = misfit64(med64)
+        med64[name][j, i] = base
+        d = (jp - jm) / (2 * h)
+        adj = g64[planes[name], j, i].item()
+        fd.append({"plane": name, "i": int(i), "j": int(j), "fd": d, "adjoint": adj,
+                   "rel_err": abs(d - adj) / max(abs(d), 1e-300)})
+    p64.close()
+    err32 = {name: float(((g1_32[k] - g64[k]).norm() / g64[k].norm()).item()) for name, k in planes.items()}
+    rel = [f["rel_err"] for f in fd]
+    return {"workload": f"vti-1024x512-nt{true.nt}-f32-gradient-{nshots}shots (start model smoothed 100 m)",
+            "shots": nshots, "seconds": sec, "shots_per_s": nshots / sec,
+            "gpts": nshots * true.nx * true.nz * true.nt / sec / 1e9, "misfit": J,
+            "grad_finite": bool(torch.isfinite(g).all().item()),
+            "fd_check": {"reference": "central differences (h = 1e-3 of the cell) of the FP64 GPU forward misfit, "
+                                      "shot 1, 20 seeded cells in the top decile of |g|",
+                         "max_rel_err": max(rel), "median_rel_err": float(np.median(rel)), "cells": fd},
+            "f32_vs_f64_rel_l2": err32}
 
 
 def measure_accuracy(a, w, plan, med, st, traces, dev):
@@ -631,7 +700,7 @@ def run_ours(a):
         out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
         out["batched_small"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=True)
     if not a.no_grad and rank == 0:
-        out["gradient"] = measure_gradient(a, dev)
+        out["gradient"] = measure_gradient_c4(a, dev)
     if not a.no_serve and rank == 0 and world == 1:
         # the server allocates its own device buffers: hand back torch's cache
         torch.cuda.empty_cache()
