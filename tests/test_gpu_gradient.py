@@ -163,8 +163,8 @@ def test_gradient_single_cells(oracle_lib, kind):
 def test_checkpoint_interval_and_precision(oracle_lib, kind):
     w = _vti(nt=200) if kind == "vti" else _tti(nt=200)
     obs, _ = oracle_lib.run(_truth(w), precision="f64")
-    J0, g0 = _gpu_gradient(w, obs, K=0)
-    for K in (1, 7, w.nt):
+    J0, g0 = _gpu_gradient(w, obs, K=0)  # every state kept in HBM: no recompute
+    for K in (1, 7, 15, w.nt):
         J, g = _gpu_gradient(w, obs, K=K)
         assert J == J0 and np.array_equal(g, g0), K
     J32, g32 = _gpu_gradient(w, obs, precision="f32")
@@ -366,3 +366,26 @@ def test_gradient_equals_oracle_adjoint(oracle_lib, kind, fs, force):
             assert not np.any(g[n]), k
             continue
         assert rel_l2(g[n], ref) <= 1e-10, (k, rel_l2(g[n], ref))
+
+
+def test_kept_states_reused_across_calls(oracle_lib):
+    """One plan, gradients with every state kept (K = 0), then checkpointed
+    (K = 7), a forward solve through vi_forward_host (which reuses the
+    workspace), then kept again: all bitwise equal; the kept states' zero
+    cells are set up again whenever the workspace was used otherwise."""
+    w = _vti(nt=120)
+    obs, _ = oracle_lib.run(_truth(w), precision="f64")
+    plan = StepPlan.for_workload(w, "f64")
+    med = plan.medium_to_device(w.medium)
+    wav = torch.as_tensor(w.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
+    obs_d = torch.as_tensor(obs, dtype=plan.dtype, device=plan.device).contiguous()
+    runs = []
+    for K in (0, 0, 7, "host", 0):
+        if K == "host":
+            plan.forward_host(w.medium, w.sources, w.wavelets, w.receivers, w.nt)
+            continue
+        J, g = misfit_gradient(plan, med, w.sources, wav, w.receivers, obs_d, checkpoint_every=K)
+        runs.append((J, g.cpu().numpy()))
+    plan.close()
+    for J, g in runs[1:]:
+        assert J == runs[0][0] and np.array_equal(g, runs[0][1])

@@ -940,25 +940,39 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   if (!grad) return set_error(VI_ERR_ARG, "gradient: grad buffer is NULL");
   if (nt <= 0) return set_error(VI_ERR_ARG, "gradient: nt must be positive");
   if ((rc = cuda_check(cudaSetDevice(p->device), "cudaSetDevice"))) return rc;
-  if (K <= 0) K = (int)std::ceil(std::sqrt((double)nt));
-  if (K > nt) K = nt;
-  const int nck = (nt + K - 1) / K;
   const long long np = (long long)c.nx * c.nz;
   const int N = c.nsls;
   const long long slot = Slot<T>::size(np, p->psix_plane, p->psiz_plane, N);
-  // workspace: checkpoints | segment (K + 1 slots) | adjoint slot | scratch (4 rbar/dbar, q, 2 h, 6 plain
-  // (TTI: also the forward effective rates of the adjoint sweep), TTI: 3 effective-rate adjoints, q15, q35) |
-  // traces
   const int nrec = shot->nrec;
   const long long ntr = 2LL * nrec * nt;
   const long long scratch = 4 * np + np + 2 * np + 6 * np + (tti ? 5 * np : 0);
-  const size_t need = sizeof(T) * ((size_t)(nck + K + 2) * slot + scratch + ntr) + 64;
+  // K = 0: every state of the forward sweep kept in HBM when the sweep fits
+  // in 60 % of the device's memory and in what is free (1024 x 512 x 3000
+  // VTI FP32: 88 GB), so the adjoint reads each step's states and nothing
+  // is recomputed; else checkpoints every ceil(sqrt(nt)) steps
+  bool keep_all = false;
+  if (K <= 0) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+      const size_t all = sizeof(T) * ((size_t)(nt + 2) * slot + scratch + ntr) + 64;
+      const size_t avail = fr + p->fwd_bytes;
+      keep_all = all <= (size_t)(0.6 * (double)tot) && all + (2ull << 30) <= avail;
+    }
+    cudaGetLastError();
+    K = (int)std::ceil(std::sqrt((double)nt));
+  }
+  if (K > nt) K = nt;
+  const int nck = keep_all ? nt + 1 : (nt + K - 1) / K;
+  // workspace: checkpoints (keep_all: every state) | segment (K + 1 slots; none when keep_all) |
+  // adjoint slot | scratch (4 rbar/dbar, q, 2 h, 6 plain (TTI: also the forward effective rates of
+  // the adjoint sweep), TTI: 3 effective-rate adjoints, q15, q35) | traces
+  const size_t need = sizeof(T) * ((size_t)(nck + (keep_all ? 0 : K + 1) + 1) * slot + scratch + ntr) + 64;
   size_t have = p->fwd_bytes;
   if ((rc = ensure_buffer(p, &p->fwd, &have, need))) return rc;
   p->fwd_bytes = have;
   T *ck = (T *)p->fwd;
-  T *seg = ck + (size_t)nck * slot;
-  T *adj = seg + (size_t)(K + 1) * slot;
+  T *seg = keep_all ? ck : ck + (size_t)nck * slot;
+  T *adj = keep_all ? ck + (size_t)nck * slot : seg + (size_t)(K + 1) * slot;
   T *rbar = adj + slot;   // also dbar
   T *q = rbar + 4 * np;
   T *h = q + np;
@@ -1074,10 +1088,36 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   };
   // ---- forward sweep with checkpoints and traces ----
   Slot<T> cur = mk(seg);
-  // every segment slot starts at zero: cells the kernels never write (outside
-  // the update region, off the CPML strips) stay zero in all of them
-  if ((rc = cuda_check(cudaMemsetAsync(seg, 0, (size_t)(K + 1) * sbytes, st), "zero segment"))) return rc;
-  {
+  // every state slot starts at zero: cells the kernels never write (outside
+  // the update region, off the CPML strips) stay zero in all of them.  The
+  // kept states are zeroed once per layout of the plan's buffer (the key
+  // is cleared by any other user of the buffer), so slot 0, never written,
+  // stays the state at rest
+  const unsigned long long zkey = keep_all ? ((unsigned long long)nt << 32) ^ (unsigned long long)slot ^
+                                                 ((unsigned long long)sizeof(T) << 60) ^ (uintptr_t)p->fwd
+                                           : 0;
+  if (keep_all && p->grad_zero_key != zkey) {
+    if ((rc = cuda_check(cudaMemsetAsync(ck, 0, (size_t)nck * sbytes, st), "zero kept states"))) return rc;
+    p->grad_zero_key = zkey;
+  } else if (!keep_all) {
+    p->grad_zero_key = 0;
+    if ((rc = cuda_check(cudaMemsetAsync(seg, 0, (size_t)(K + 1) * sbytes, st), "zero segment"))) return rc;
+  }
+  if (keep_all) {
+    NvtxRange nr("vi_gradient: forward sweep, every state kept");
+    for (int it = 0; it < nt; ++it) {
+      T *nxt = ck + (size_t)(it + 1) * slot;
+      if (use_split) {
+        const Slot<T> out = mk(nxt);
+        if ((rc = fwd_step(mk(ck + (size_t)it * slot), it, tr, it > 0, &out))) return rc;
+      } else {
+        if ((rc = cuda_check(cudaMemcpyAsync(nxt, ck + (size_t)it * slot, sbytes, cudaMemcpyDeviceToDevice, st),
+                             "state copy")))
+          return rc;
+        if ((rc = fwd_step(mk(nxt), it, tr, false))) return rc;
+      }
+    }
+  } else {
     NvtxRange nr("vi_gradient: forward sweep");
     for (int it = 0; it < nt; ++it) {
       if (it % K == 0)
@@ -1134,14 +1174,16 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     const cudaError_t e = launch_pdl(kernel, g, b, 0, st, true, args...);
     if (e != cudaSuccess && !lrc) lrc = cuda_check(e, "adjoint launch");
   };
-  for (int qseg = nck - 1; qseg >= 0; --qseg) {
-    const int s0 = qseg * K, s1 = std::min(nt, s0 + K);
+  // keep_all: one segment of nt steps whose states are all kept
+  for (int qseg = keep_all ? 0 : nck - 1; qseg >= 0; --qseg) {
+    const int s0 = keep_all ? 0 : qseg * K, s1 = keep_all ? nt : std::min(nt, s0 + K);
     // recompute the segment: seg[k] = state before step s0 + k
-    if ((rc = cuda_check(cudaMemcpyAsync(seg, ck + (size_t)qseg * slot, sbytes, cudaMemcpyDeviceToDevice, st),
+    if (!keep_all &&
+        (rc = cuda_check(cudaMemcpyAsync(seg, ck + (size_t)qseg * slot, sbytes, cudaMemcpyDeviceToDevice, st),
                          "restore checkpoint")))
       return rc;
     NvtxRange nr_seg("vi_gradient: segment recompute and adjoint");
-    for (int k = 0; k < s1 - s0; ++k) {
+    for (int k = 0; !keep_all && k < s1 - s0; ++k) {
       T *nxt = seg + (size_t)(k + 1) * slot;
       if (use_split) {
         // straight from slot k into slot k + 1 (no copy of the state)

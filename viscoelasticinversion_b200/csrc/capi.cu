@@ -637,6 +637,7 @@ static int forward_host_impl(vi_plan *p, const vi_medium *mh, int nsrc, const vi
                        2 * (size_t)nrec * nt * sizeof(T) + 256 * 4;
   rc = ensure_buffer(p, &p->fwd, &p->fwd_bytes, bytes);
   if (rc) return rc;
+  p->grad_zero_key = 0;  // the gradient's kept states are overwritten
   T *base = (T *)p->fwd;
   const void *hp[8] = {mh->rho, mh->c11, mh->c13, mh->c15, mh->c33, mh->c35, mh->c55, mh->tau};
   vi_medium md;

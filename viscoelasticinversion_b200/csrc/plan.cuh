@@ -39,9 +39,12 @@ struct vi_plan {
   void *wave_ctl = nullptr;
   size_t wave_ctl_bytes = 0;
   int wave_k = 0, wave_d = 0;
-  // forward_host buffers (device, grown on demand)
+  // forward_host buffers and the gradient's workspace (device, grown on demand)
   void *fwd = nullptr;
   size_t fwd_bytes = 0;
+  // layout of the gradient's kept states whose never-written cells are
+  // known zero (0: none)
+  unsigned long long grad_zero_key = 0;
   size_t bytes = 0;  // device bytes held
   // host copies of the CPML tables in double precision
   std::vector<double> htx, htz;

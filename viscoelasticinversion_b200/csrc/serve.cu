@@ -26,6 +26,7 @@
 // one vi_step call).  Latency is measured from submit to the moment the
 // results are in the caller's host buffers.
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -259,7 +260,10 @@ int advance(vi_server *s, Req &q, bool *finished) {
   int rc;
   if (r.kind == VI_REQ_GRADIENT) {
     double J = 0;
-    if ((rc = vi_gradient(q.plan, &q.md, &q.shot, r.nt, q.obs_dev, 0, 0, q.grad_dev, &J, q.st))) return rc;
+    // checkpoints every ceil(sqrt(nt)) steps, as the admission estimate
+    // assumes (checkpoint_every 0 may keep every state in HBM)
+    const int K = (int)std::ceil(std::sqrt((double)r.nt));
+    if ((rc = vi_gradient(q.plan, &q.md, &q.shot, r.nt, q.obs_dev, K, 0, q.grad_dev, &J, q.st))) return rc;
     const size_t np = (size_t)r.cfg.nx * r.cfg.nz;
     if ((rc = cuda_check(cudaMemcpyAsync(r.grad_host, q.grad_dev, 8 * np * sizeof(double), cudaMemcpyDeviceToHost,
                                          q.st),
