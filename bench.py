@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--batch-shots", type=int, default=64)
+    p.add_argument("--batch-set", default="both", choices=["both", "c3", "small"],
+                   help="which gathers the batch leg times")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-grad", action="store_true")
     p.add_argument("--grad-nt", type=int, default=3000)
@@ -697,8 +699,10 @@ def run_ours(a):
         out["gpu_launches"] += a.steps * kernels
 
     if not a.no_batch:
-        out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
-        out["batched_small"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=True)
+        if a.batch_set in ("both", "c3"):
+            out["batched"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world)
+        if a.batch_set in ("both", "small"):
+            out["batched_small"] = measure_batch(a, dev, stream, max_over_ranks, barrier, world, small=True)
     if not a.no_grad and rank == 0:
         out["gradient"] = measure_gradient_c4(a, dev)
     if not a.no_serve and rank == 0 and world == 1:
