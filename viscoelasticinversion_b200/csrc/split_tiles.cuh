@@ -8,6 +8,7 @@
 #include <cstdint>
 
 #include "afda.cuh"
+#include "cpml4.cuh"
 #include "fused_tma.cuh"
 #include "pdl.cuh"
 #include "split.cuh"
@@ -37,36 +38,12 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
   Q4<T> dxx = dps4(hxx, a.Dx), dxxz = dms4(hxz, a.Dx);
-  if (xstrip) {  // CPML, cell by cell
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int gi = gi0 + k;
-      const int xs = strip_x(gi, nx, a.Lx, a.Rx);
-      if (xs >= 0) {
-        const T *tb = a.tx;
-        const long long o = (long long)gj * a.wx + xs;
-        const T p0 = tb[T_BH * nx + gi] * a.psix[PX_SXX * a.psix_plane + o] + tb[T_AH * nx + gi] * dxx.v[k];
-        const T p1 = tb[T_B * nx + gi] * a.psix[PX_SXZ * a.psix_plane + o] + tb[T_A * nx + gi] * dxxz.v[k];
-        psix_o[PX_SXX * a.psix_plane + o] = p0;
-        psix_o[PX_SXZ * a.psix_plane + o] = p1;
-        dxx.v[k] = dxx.v[k] * tb[T_IKH * nx + gi] + p0;
-        dxxz.v[k] = dxxz.v[k] * tb[T_IK * nx + gi] + p1;
-      }
-    }
-  }
-  if (zs >= 0) {
-    const T *tb = a.tz;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const long long o = (long long)zs * nx + gi0 + k;
-      const T p0 = tb[T_B * nz + gj] * a.psiz[PZ_SXZ * a.psiz_plane + o] + tb[T_A * nz + gj] * zxz.v[k];
-      const T p1 = tb[T_BH * nz + gj] * a.psiz[PZ_SZZ * a.psiz_plane + o] + tb[T_AH * nz + gj] * zzz.v[k];
-      psiz_o[PZ_SXZ * a.psiz_plane + o] = p0;
-      psiz_o[PZ_SZZ * a.psiz_plane + o] = p1;
-      zxz.v[k] = zxz.v[k] * tb[T_IK * nz + gj] + p0;
-      zzz.v[k] = zzz.v[k] * tb[T_IKH * nz + gj] + p1;
-    }
-  }
+  if (xstrip)
+    cpml_x4(a, gi0, gj, CpmlRows{PX_SXX, T_BH, T_AH, T_IKH}, CpmlRows{PX_SXZ, T_B, T_A, T_IK}, a.psix, psix_o, true,
+            dxx, dxxz);
+  if (zs >= 0)
+    cpml_z4(a, zs, gi0, gj, CpmlRows{PZ_SXZ, T_B, T_A, T_IK}, CpmlRows{PZ_SZZ, T_BH, T_AH, T_IKH}, a.psiz, psiz_o,
+            true, zxz, zzz);
   const Q4<T> sx = add4(r0, Q4<T>{{r0.v[1], r0.v[2], r0.v[3], r4}}), sz = add4(r0, r1);
   Q4<T> bx, bz;
 #pragma unroll
@@ -379,38 +356,12 @@ __device__ __forceinline__ void split_stress_tile(const StepArgs<T> &a, const Fu
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
   const bool surf = x.fs && gj == L;
   Q4<T> rxx = dms4(hvx, a.Dx), dxvz = dps4(hvz, a.Dx), rzz = zvz, dzvx = zvx;
-  if (xstrip) {  // CPML, cell by cell
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int gi = gi0 + k;
-      const int xs = strip_x(gi, nx, a.Lx, a.Rx);
-      if (xs >= 0) {
-        const T *tb = a.tx;
-        const long long o = (long long)gj * a.wx + xs;
-        T *q = OOP ? a.psix_o : a.psix;
-        const T p0 = tb[T_B * nx + gi] * a.psix[PX_VX * a.psix_plane + o] + tb[T_A * nx + gi] * rxx.v[k];
-        const T p1 = tb[T_BH * nx + gi] * a.psix[PX_VZ * a.psix_plane + o] + tb[T_AH * nx + gi] * dxvz.v[k];
-        q[PX_VX * a.psix_plane + o] = p0;
-        q[PX_VZ * a.psix_plane + o] = p1;
-        rxx.v[k] = rxx.v[k] * tb[T_IK * nx + gi] + p0;
-        dxvz.v[k] = dxvz.v[k] * tb[T_IKH * nx + gi] + p1;
-      }
-    }
-  }
-  if (zs >= 0) {
-    const T *tb = a.tz;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const long long o = (long long)zs * nx + gi0 + k;
-      T *q = OOP ? a.psiz_o : a.psiz;
-      const T p0 = tb[T_B * nz + gj] * a.psiz[PZ_VZ * a.psiz_plane + o] + tb[T_A * nz + gj] * rzz.v[k];
-      const T p1 = tb[T_BH * nz + gj] * a.psiz[PZ_VX * a.psiz_plane + o] + tb[T_AH * nz + gj] * dzvx.v[k];
-      q[PZ_VZ * a.psiz_plane + o] = p0;
-      q[PZ_VX * a.psiz_plane + o] = p1;
-      rzz.v[k] = rzz.v[k] * tb[T_IK * nz + gj] + p0;
-      dzvx.v[k] = dzvx.v[k] * tb[T_IKH * nz + gj] + p1;
-    }
-  }
+  if (xstrip)
+    cpml_x4(a, gi0, gj, CpmlRows{PX_VX, T_B, T_A, T_IK}, CpmlRows{PX_VZ, T_BH, T_AH, T_IKH}, a.psix,
+            OOP ? a.psix_o : a.psix, true, rxx, dxvz);
+  if (zs >= 0)
+    cpml_z4(a, zs, gi0, gj, CpmlRows{PZ_VZ, T_B, T_A, T_IK}, CpmlRows{PZ_VX, T_BH, T_AH, T_IKH}, a.psiz,
+            OOP ? a.psiz_o : a.psiz, true, rzz, dzvx);
   const Q4<T> rxz = add4(dzvx, dxvz);
   // ---- SLS effective rates and the stress update (4 cells at once)
   const T dt = a.dt;

@@ -18,6 +18,7 @@
 #include <cstdint>
 
 #include "afda.cuh"
+#include "cpml4.cuh"
 #include "pdl.cuh"
 #include "plan.cuh"
 #include "split.cuh"
@@ -61,41 +62,13 @@ __device__ __forceinline__ void tti_rates4(const StepArgs<T> &a, const T *s_vx, 
   }
   const int nx = a.nx, nz = a.nz;
   Q4<T> dxvx = dms4(hvx, a.Dx), dxvz = dps4(hvz, a.Dx), dzvz = zvz, dzvx = zvx;
-  if (gi0 < a.Lx || gi0 + 3 >= nx - a.Rx) {  // CPML, cell by cell
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int gi = gi0 + k;
-      const int xs = strip_x(gi, nx, a.Lx, a.Rx);
-      if (xs >= 0) {
-        const T *tb = a.tx;
-        const long long o = (long long)gj * a.wx + xs;
-        const T p0 = tb[T_B * nx + gi] * a.psix[PX_VX * a.psix_plane + o] + tb[T_A * nx + gi] * dxvx.v[k];
-        const T p1 = tb[T_BH * nx + gi] * a.psix[PX_VZ * a.psix_plane + o] + tb[T_AH * nx + gi] * dxvz.v[k];
-        if (own) {
-          a.psix_o[PX_VX * a.psix_plane + o] = p0;
-          a.psix_o[PX_VZ * a.psix_plane + o] = p1;
-        }
-        dxvx.v[k] = dxvx.v[k] * tb[T_IK * nx + gi] + p0;
-        dxvz.v[k] = dxvz.v[k] * tb[T_IKH * nx + gi] + p1;
-      }
-    }
-  }
+  if (gi0 < a.Lx || gi0 + 3 >= nx - a.Rx)
+    cpml_x4(a, gi0, gj, CpmlRows{PX_VX, T_B, T_A, T_IK}, CpmlRows{PX_VZ, T_BH, T_AH, T_IKH}, a.psix, a.psix_o, own,
+            dxvx, dxvz);
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
-  if (zs >= 0) {
-    const T *tb = a.tz;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const long long o = (long long)zs * nx + gi0 + k;
-      const T p0 = tb[T_B * nz + gj] * a.psiz[PZ_VZ * a.psiz_plane + o] + tb[T_A * nz + gj] * dzvz.v[k];
-      const T p1 = tb[T_BH * nz + gj] * a.psiz[PZ_VX * a.psiz_plane + o] + tb[T_AH * nz + gj] * dzvx.v[k];
-      if (own) {
-        a.psiz_o[PZ_VZ * a.psiz_plane + o] = p0;
-        a.psiz_o[PZ_VX * a.psiz_plane + o] = p1;
-      }
-      dzvz.v[k] = dzvz.v[k] * tb[T_IK * nz + gj] + p0;
-      dzvx.v[k] = dzvx.v[k] * tb[T_IKH * nz + gj] + p1;
-    }
-  }
+  if (zs >= 0)
+    cpml_z4(a, zs, gi0, gj, CpmlRows{PZ_VZ, T_B, T_A, T_IK}, CpmlRows{PZ_VX, T_BH, T_AH, T_IKH}, a.psiz, a.psiz_o,
+            own, dzvz, dzvx);
   rxx = dxvx;
   rzz = dzvz;
   rxz = add4(dzvx, dxvz);

@@ -55,6 +55,22 @@ __device__ __forceinline__ T lane4(const Q4<T> &q, int k) {
 // source term with the same bits
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// CPML memory and rate of one cell, with their roundings fixed (so the
+// 4-cell and the cell-by-cell forms give the same bits): psi' = a d + b psi
+// (the product b psi rounded, then one fused multiply-add), d' = d ik + psi'.
+template <typename T>
+__device__ __forceinline__ T cpml_mem(T b, T psi, T a, T d) {
+  return fma_rn(a, d, mul_rn(b, psi));
+}
+template <typename T>
+__device__ __forceinline__ T cpml_rate(T d, T ik, T p) {
+  return fma_rn(d, ik, p);
+}
 template <typename T>
 __device__ __forceinline__ void add_lane4(Q4<T> &q, int k, T d) {
 #pragma unroll
