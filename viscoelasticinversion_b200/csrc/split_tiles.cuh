@@ -33,7 +33,7 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
                                                  int gi0, int gj, long long g, const Q4<T> &vxi,
                                                  const Q4<T> &vzi, const Q4<T> &r0, const Q4<T> &r1, T r4,
                                                  const T (&hxx)[12], const T (&hxz)[12], Q4<T> zxz,
-                                                 Q4<T> zzz, T *psix_o, T *psiz_o) {
+                                                 Q4<T> zzz, T *psix_o, T *psiz_o, int e0, int e1) {
   const int nx = a.nx, nz = a.nz;
   const int zs = strip_z(gj, nz, a.Tz, a.Bz);
   const bool xstrip = gi0 < a.Lx || gi0 + 3 >= nx - a.Rx;
@@ -54,8 +54,7 @@ __device__ __forceinline__ void split_vel_finish(const StepArgs<T> &a, const Fus
   const Q4<T> dt4 = splat4<T>(a.dt);
   Q4<T> vxn = fma4(mul4(dt4, bx), add4(dxx, zxz), vxi);
   Q4<T> vzn = fma4(mul4(dt4, bz), add4(dxxz, zzz), vzi);
-  const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
-  for (int e = e0; e < e1; ++e) {  // force sources of this tile (listed first)
+  for (int e = e0; e < e1; ++e) {  // force sources of this tile (listed first; e0, e1 loaded early)
     const int4 en = x.tile_ent[e];
     if (en.w > TL_FORCE_Z) break;
     if (en.y != gj || en.x < gi0 || en.x >= gi0 + 4) continue;
@@ -110,6 +109,7 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
   if (gi0 >= xe || gj >= ze) return;
   const long long g = (long long)gj * nx + gi0;
   const Q4<T> vxi = ldc4(a.vx + g), vzi = ldc4(a.vz + g);
+  const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];
   const Q4<T> r0 = ldg4(a.rho + g), r1 = ldg4(a.rho + g + nx);
   const T r4 = __ldg(a.rho + g + 4);
   T hxx[12], hxz[12];
@@ -141,7 +141,8 @@ __device__ __forceinline__ void split_vel_tile(const StepArgs<T> &a, const Fused
     zxz = afda4<0>(a, qs, [&](int m) { return ldg4(a.sxz + (long long)(L + m) * nx + gi0); });
     if (qs < 3) zzz = afda4<1>(a, qs, [&](int m) { return ldg4(a.szz + (long long)(L + 1 + m) * nx + gi0); });
   }
-  split_vel_finish<T, PP, OOP, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+  split_vel_finish<T, PP, OOP, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o,
+                                     e0, e1);
 }
 
 // Tile height of the TMA-staged velocity pass (64 x 8: 34.8 Gpt/s on the
@@ -210,6 +211,7 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
     r1 = ldg4(a.rho + g + nx);
     r4 = __ldg(a.rho + g + 4);
   }
+  const int e0 = x.tile_off[tile], e1 = x.tile_off[tile + 1];  // the tile's sources, while the boxes land
   pdl_wait();  // every thread, before its first store
   const bool ok = mbar_wait_bounded(bar, 0, 1u << 22);
   if (__syncthreads_or(!ok)) {
@@ -243,7 +245,8 @@ __device__ __forceinline__ void split_vel_tma_tile(const StepArgs<T> &a, const F
     zxz = afda4<0>(a, qs, [&](int m) { return lds4(s_sxz + (m + 4) * WX + lx + 4); });
     if (qs < 3) zzz = afda4<1>(a, qs, [&](int m) { return lds4(s_szz + (m + 5) * WZ + lx); });
   }
-  split_vel_finish<T, PP, false, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o, psiz_o);
+  split_vel_finish<T, PP, false, HINT>(a, x, tile, gi0, gj, g, vxi, vzi, r0, r1, r4, hxx, hxz, zxz, zzz, psix_o,
+                                       psiz_o, e0, e1);
 }
 
 // ------------------------------------------------------------------ stress
