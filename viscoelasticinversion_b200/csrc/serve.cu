@@ -15,7 +15,8 @@
 //    gradient), so a short request that arrives while a long one runs
 //    preempts it at the next slice boundary (shortest remaining work
 //    first, which minimises mean latency);
-//  * gradient requests run whole when their turn comes (one vi_gradient);
+//  * gradient requests run whole when their turn comes (one vi_gradient),
+//    on at most L - 1 of the L lanes while a forward request waits;
 //  * lanes: each lane takes the next slice of the best idle resident
 //    request and issues it on that request's stream; with L lanes the L
 //    requests with the least remaining work advance at the same time (a
@@ -308,11 +309,22 @@ bool can_admit(const vi_server *s) {
          s->used + s->queue.front()->footprint <= s->cfg.hbm_budget_bytes;
 }
 
-// the idle resident request the policy picks next (nullptr if none)
+// the idle resident request the policy picks next (nullptr if none).  A
+// gradient holds its lane for its whole length, so while lanes - 1 lanes
+// run gradients an idle forward request goes first: the forward stream is
+// never left without a lane
 std::shared_ptr<Req> pick_idle(vi_server *s) {
+  int grads = 0;
+  bool idle_fwd = false;
+  for (auto &q : s->active) {
+    if (q->busy && q->rq.kind == VI_REQ_GRADIENT) ++grads;
+    if (!q->busy && q->rq.kind != VI_REQ_GRADIENT) idle_fwd = true;
+  }
+  const bool hold_grads = s->cfg.lanes > 1 && grads >= s->cfg.lanes - 1 && idle_fwd;
   std::shared_ptr<Req> best;
   for (auto &q : s->active) {
     if (q->busy) continue;
+    if (hold_grads && q->rq.kind == VI_REQ_GRADIENT) continue;
     if (!best) {
       best = q;
     } else if (s->cfg.policy == VI_SERVE_ROUND_ROBIN ? q->last_turn < best->last_turn
