@@ -1016,10 +1016,12 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
   using SG = SplitGeom<T>;
   StepArgs<T> probe = a;
   bind(probe, mk(seg));
-  // TTI sweeps run the plain path (the TTI split pass has no out-of-place
-  // form); the 4-cell transposed derivatives only need aligned planes
+  // TTI sweeps step out of place only (the TTI stress pass reads M and psi
+  // on a ring of neighbouring cells, so it writes them to the other slot);
+  // the 4-cell transposed derivatives only need aligned planes
   const bool split_ok = split_eligible<T>(p, probe);
-  const bool use_split = split_ok && !tti;
+  const bool use_split = split_ok;
+  using STG = SplitTtiGeom<T>;
   using SS = SplitStressGeom<T>;
   FusedExtras<T> fx{}, fxs{};
   SplitMaps ms{};
@@ -1030,7 +1032,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     std::vector<int> off, soff;
     std::vector<int4> ent, sent;
     build_tile_lists(c.nx, c.nz, SG::TX, SG::TZ, 0, shot, off, ent, ntx, ntz);
-    build_tile_lists(c.nx, c.nz, SS::TX, SS::TZ, 0, shot, soff, sent, sntx, sntz);
+    build_tile_lists(c.nx, c.nz, tti ? STG::TX : SS::TX, tti ? STG::TZ : SS::TZ, 0, shot, soff, sent, sntx, sntz);
     const int nvoff = (int)off.size();
     for (int v : soff) off.push_back(v + (int)ent.size());
     ent.insert(ent.end(), sent.begin(), sent.end());
@@ -1068,6 +1070,29 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
       return VI_OK;
     }
     StepArgs<T> b = a;
+    if (tti) {
+      // v and sigma copied into the output slot and stepped there in place;
+      // M and psi from the input slot to the output one
+      if (!out) return set_error(VI_ERR_ARG, "gradient: the TTI split step runs out of place");
+      int r2 = cuda_check(cudaMemcpyAsync(out->vx(), sl.vx(), 5 * (size_t)np * sizeof(T), cudaMemcpyDeviceToDevice, st),
+                          "state copy");
+      bind(b, *out);
+      b.m = sl.m();
+      b.mstride = np;
+      b.m_o = out->m();
+      b.mstride_o = np;
+      b.psix = p->wx ? sl.psix() : nullptr;
+      b.psiz = p->hz ? sl.psiz() : nullptr;
+      b.psix_o = p->wx ? out->psix() : nullptr;
+      b.psiz_o = p->hz ? out->psiz() : nullptr;
+      fx.it = fxs.it = it;
+      fx.traces = fxs.traces = traces;
+      if (!r2) r2 = encode_map(&ms.a, out->vx(), (int)sizeof(T), c.nx, c.nz, 1, 0, STG::BW, STG::BH, 1);
+      if (!r2) r2 = encode_map(&ms.b, out->vz(), (int)sizeof(T), c.nx, c.nz, 1, 0, STG::BW, STG::BH, 1);
+      if (!r2) r2 = launch_split_vel<T>(b, fx, ntiles, st, false);
+      if (!r2) r2 = launch_split_stress_tti<T>(b, fxs, ms, sntiles, st, true);
+      return r2;
+    }
     bind(b, sl);
     if (out) {
       b.vx_o = out->vx(); b.vz_o = out->vz();
@@ -1121,10 +1146,17 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     NvtxRange nr("vi_gradient: forward sweep");
     for (int it = 0; it < nt; ++it) {
       if (it % K == 0)
-        if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, seg, sbytes, cudaMemcpyDeviceToDevice, st),
+        if ((rc = cuda_check(cudaMemcpyAsync(ck + (size_t)(it / K) * slot, cur.base, sbytes,
+                                             cudaMemcpyDeviceToDevice, st),
                              "checkpoint")))
           return rc;
-      if ((rc = fwd_step(cur, it, tr, it % K != 0))) return rc;
+      if (tti && use_split) {  // out of place: between the segment's first two slots
+        const Slot<T> nxt = mk(cur.base == seg ? seg + slot : seg);
+        if ((rc = fwd_step(cur, it, tr, false, &nxt))) return rc;
+        cur = nxt;
+      } else if ((rc = fwd_step(cur, it, tr, it % K != 0))) {
+        return rc;
+      }
     }
   }
   if (shot->traces_dev && shot->traces_nt >= nt) {
