@@ -116,6 +116,33 @@ def test_short_request_finishes_while_a_gradient_runs():
     assert np.array_equal(f.traces, _direct(small, "f32"))
 
 
+def test_gradient_is_sliced_on_one_lane():
+    """Gradient requests advance in slices like forward ones: on a single
+    lane a small forward solve submitted while a long gradient runs still
+    completes first, and the sliced gradient equals the direct call."""
+    big = media.homogeneous_iso(nx=512, nz=256, nt=1200, pml=20, nrec=16, src=(256, 60))
+    obs = np.zeros((2, len(big.receivers), big.nt), np.float32)
+    small = media.homogeneous_iso(nx=96, nz=80, nt=60, pml=12, nrec=8, src=(40, 30))
+    srv = Server(lanes=1, slice_steps=256)
+    g = srv.submit_gradient(big, obs, "f32")
+    import time
+    t0 = time.perf_counter()
+    while srv.poll(g)[0] != "running" and time.perf_counter() - t0 < 30:
+        time.sleep(0.002)
+    f = srv.submit_forward(small)
+    assert srv.wait(f, 60.0) == "done"
+    assert srv.poll(g)[0] == "running"
+    assert srv.wait(g, 120.0) == "done"
+    srv.stop()
+    plan = StepPlan.for_workload(big, "f32")
+    med = plan.medium_to_device(big.medium)
+    wav = torch.as_tensor(big.wavelets, dtype=plan.dtype, device=plan.device).contiguous()
+    obs_d = torch.as_tensor(obs, dtype=plan.dtype, device=plan.device).contiguous()
+    J, gd = misfit_gradient(plan, med, big.sources, wav, big.receivers, obs_d)
+    plan.close()
+    assert g.misfit[0] == J and np.array_equal(g.grad, gd.cpu().numpy())
+
+
 def test_budget_admission():
     w = media.homogeneous_iso(nx=96, nz=80, nt=120, pml=12, nrec=8, src=(40, 30))
     small = Server(hbm_budget_bytes=1 << 20)

@@ -1111,6 +1111,11 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
     if (!r2) r2 = launch_split_stress<T>(c.medium, b, fxs, ms, sntiles, st, true);
     return r2;
   };
+  // the caller's hook after every enqueued step (a server's slicing)
+  auto yield = [&](int units) -> int {
+    if (p->yield_fn && p->yield_fn(p->yield_ctx, units)) return set_error(VI_ERR_STATE, "gradient: stopped");
+    return VI_OK;
+  };
   // ---- forward sweep with checkpoints and traces ----
   Slot<T> cur = mk(seg);
   // every state slot starts at zero: cells the kernels never write (outside
@@ -1141,6 +1146,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
           return rc;
         if ((rc = fwd_step(mk(nxt), it, tr, false))) return rc;
       }
+      if ((rc = yield(1))) return rc;
     }
   } else {
     NvtxRange nr("vi_gradient: forward sweep");
@@ -1157,6 +1163,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
       } else if ((rc = fwd_step(cur, it, tr, it % K != 0))) {
         return rc;
       }
+      if ((rc = yield(1))) return rc;
     }
   }
   if (shot->traces_dev && shot->traces_nt >= nt) {
@@ -1227,6 +1234,7 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
           return rc;
         if ((rc = fwd_step(mk(nxt), s0 + k, nullptr, false))) return rc;
       }
+      if ((rc = yield(1))) return rc;
     }
     for (int it = s1 - 1; it >= s0; --it) {
       const Slot<T> x0 = mk(seg + (size_t)(it - s0) * slot), x1 = mk(seg + (size_t)(it - s0 + 1) * slot);
@@ -1277,6 +1285,8 @@ static int gradient_impl(vi_plan *p, const vi_medium *m, const vi_shot *shot, in
         lc(k_div_t4<T>, gA4, blk, A, ab, (const T *)rbar);
       else
         lc(k_div_t<T>, gA, blk, A, ab, (const T *)rbar);
+      if (lrc) return lrc;
+      if ((rc = yield(2))) return rc;
     }
   }
   if (lrc) return lrc;

@@ -45,6 +45,11 @@ struct vi_plan {
   // layout of the gradient's kept states whose never-written cells are
   // known zero (0: none)
   unsigned long long grad_zero_key = 0;
+  // called by vi_gradient on its own thread after every step it enqueues
+  // (units: 1 per forward or recompute step, 2 per adjoint step); a
+  // server uses it to run a gradient in slices.  Nonzero: stop.
+  int (*yield_fn)(void *ctx, int units) = nullptr;
+  void *yield_ctx = nullptr;
   size_t bytes = 0;  // device bytes held
   // host copies of the CPML tables in double precision
   std::vector<double> htx, htz;

@@ -15,8 +15,10 @@
 //    gradient), so a short request that arrives while a long one runs
 //    preempts it at the next slice boundary (shortest remaining work
 //    first, which minimises mean latency);
-//  * gradient requests run whole when their turn comes (one vi_gradient),
-//    on at most L - 1 of the L lanes while a forward request waits;
+//  * gradient requests run in slices too: vi_gradient runs on a thread of
+//    the request's own that yields after every slice_steps step units (a
+//    forward or recompute step 1, an adjoint step 2), and while L - 1 lanes
+//    run gradient slices an idle forward request goes first;
 //  * lanes: each lane takes the next slice of the best idle resident
 //    request and issues it on that request's stream; with L lanes the L
 //    requests with the least remaining work advance at the same time (a
@@ -26,6 +28,7 @@
 // depend on what else is resident (the sliced stepping is bitwise equal to
 // one vi_step call).  Latency is measured from submit to the moment the
 // results are in the caller's host buffers.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -45,6 +48,38 @@ using Clock = std::chrono::steady_clock;
 
 namespace vb {
 namespace {
+
+// A gradient request runs vi_gradient on a thread of its own, which yields
+// after every slice (plan yield hook): a lane that picks the request hands
+// it a budget of slice_steps step units and waits until the thread has
+// enqueued them or finished, so a gradient holds a lane one slice at a
+// time, as a forward request does.
+struct GradRun {
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;
+  long long budget = 0;   // units the thread may still enqueue
+  bool running = false;   // a lane handed it a budget and waits for the yield
+  bool abort = false;     // the request is being released unfinished
+  bool done = false;
+  int rc = VI_OK;
+  std::string msg;
+  double J = 0;
+  long long units = 0;    // enqueued so far (1 per forward step, 2 per adjoint step)
+};
+
+int grad_yield(void *ctx, int units) {
+  auto *g = static_cast<GradRun *>(ctx);
+  std::unique_lock<std::mutex> lk(g->mu);
+  g->units += units;
+  g->budget -= units;
+  if (g->budget <= 0 && !g->abort) {
+    g->running = false;
+    g->cv.notify_all();
+    g->cv.wait(lk, [&] { return g->running || g->abort; });
+  }
+  return g->abort ? 1 : 0;
+}
 
 struct Req {
   uint64_t ticket = 0;
@@ -68,6 +103,7 @@ struct Req {
   cudaStream_t st = nullptr;  // the request's own stream: its slices stay in order
   bool busy = false;          // a lane is advancing it (under the server lock)
   uint64_t last_turn = 0;     // round robin: when it last got a slice
+  std::shared_ptr<GradRun> gr;  // gradient requests, once started
 };
 
 size_t esize_of(const vi_config &c) { return c.precision == VI_F64 ? 8 : 4; }
@@ -243,6 +279,15 @@ int admit(vi_server *s, Req &q) {
 }
 
 void release(vi_server *s, Req &q) {
+  if (q.gr && q.gr->th.joinable()) {  // a gradient left unfinished: stop its thread
+    {
+      std::lock_guard<std::mutex> lk(q.gr->mu);
+      q.gr->abort = true;
+      q.gr->cv.notify_all();
+    }
+    q.gr->th.join();
+  }
+  q.gr.reset();
   if (q.buf) cudaFreeAsync(q.buf, q.st);
   q.buf = nullptr;
   if (q.st) cudaStreamSynchronize(q.st);
@@ -252,19 +297,64 @@ void release(vi_server *s, Req &q) {
   q.st = nullptr;
 }
 
-// Runs the request's next slice (forward) or all of it (gradient); returns
-// true when the request is finished.
+// Runs the request's next slice; sets *finished when the request is done.
 int advance(vi_server *s, Req &q, bool *finished) {
   NvtxRange nr(q.rq.kind == VI_REQ_GRADIENT ? "vi_serve: gradient request" : "vi_serve: forward slice");
   const vi_request &r = q.rq;
   const size_t es = esize_of(r.cfg);
   int rc;
   if (r.kind == VI_REQ_GRADIENT) {
-    double J = 0;
-    // checkpoints every ceil(sqrt(nt)) steps, as the admission estimate
-    // assumes (checkpoint_every 0 may keep every state in HBM)
-    const int K = (int)std::ceil(std::sqrt((double)r.nt));
-    if ((rc = vi_gradient(q.plan, &q.md, &q.shot, r.nt, q.obs_dev, K, 0, q.grad_dev, &J, q.st))) return rc;
+    if (!q.gr) {
+      q.gr = std::make_shared<GradRun>();
+      GradRun *g = q.gr.get();
+      Req *qp = &q;
+      const int dev = s->cfg.device;
+      g->th = std::thread([g, qp, dev] {
+        cudaSetDevice(dev);
+        {
+          std::unique_lock<std::mutex> lk(g->mu);
+          g->cv.wait(lk, [&] { return g->running || g->abort; });
+        }
+        const vi_request &rr = qp->rq;
+        // checkpoints every ceil(sqrt(nt)) steps, as the admission estimate
+        // assumes (checkpoint_every 0 may keep every state in HBM)
+        const int K = (int)std::ceil(std::sqrt((double)rr.nt));
+        double J = 0;
+        int grc = VI_ERR_STATE;
+        std::string msg = "gradient: stopped";
+        if (!g->abort) {
+          qp->plan->yield_fn = grad_yield;
+          qp->plan->yield_ctx = g;
+          grc = vi_gradient(qp->plan, &qp->md, &qp->shot, rr.nt, qp->obs_dev, K, 0, qp->grad_dev, &J, qp->st);
+          qp->plan->yield_fn = nullptr;
+          qp->plan->yield_ctx = nullptr;
+          if (grc) msg = vi_last_error();
+        }
+        std::lock_guard<std::mutex> lk(g->mu);
+        g->rc = grc;
+        if (grc) g->msg = msg;
+        g->J = J;
+        g->done = true;
+        g->running = false;
+        g->cv.notify_all();
+      });
+    }
+    GradRun &g = *q.gr;
+    {
+      std::unique_lock<std::mutex> lk(g.mu);
+      g.budget = s->cfg.slice_steps;
+      g.running = true;
+      g.cv.notify_all();
+      g.cv.wait(lk, [&] { return !g.running; });
+      q.done_steps = (int)std::min<long long>(r.nt, g.units / 4);
+      if (!g.done) {
+        *finished = false;
+        return VI_OK;
+      }
+    }
+    g.th.join();
+    if (g.rc) return set_error(g.rc, g.msg);
+    const double J = g.J;
     const size_t np = (size_t)r.cfg.nx * r.cfg.nz;
     if ((rc = cuda_check(cudaMemcpyAsync(r.grad_host, q.grad_dev, 8 * np * sizeof(double), cudaMemcpyDeviceToHost,
                                          q.st),
