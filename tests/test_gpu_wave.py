@@ -94,7 +94,7 @@ def test_wave_refuses_what_it_does_not_cover():
     w = media.layered(nx=128, nz=64, nt=4, kind="vti", seed=2, pml=8, nrec=4)
     plan = StepPlan.for_workload(w, "f32")
     with pytest.raises(ViError):
-        plan.set_wave(4, 1)  # a lag below 2 would let a unit wait on a later ticket
+        plan.set_wave(4, 1)  # lags below 2 are refused (2 keeps every dependency at an earlier tau)
     plan.close()
 
 
