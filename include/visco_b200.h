@@ -271,9 +271,10 @@ int vi_batch_set_shot(vi_batch *batch, int32_t i, const vi_medium *med_dev,
  * shots to rest (fields, memory variables and CPML memory zeroed) before
  * the run proper.  Every run zeroes the CPML memory first. */
 int vi_batch_run(vi_batch *batch, int32_t flags, void *stream);
-/* Synchronizes, reports the kernel form in use (3 per shot: each shot's
- * own vi_step loop, 2 split velocity/stress pair, 1 two-stage persistent
- * fused, 0 one-stage fused) and any
+/* Synchronizes, reports the kernel form in use (4 per shot on 8
+ * concurrent streams: each shot's own vi_step loop, shots side by side, 3
+ * per shot one after the other, 2 split velocity/stress pair over all
+ * shots' tiles, 1 two-stage persistent fused, 0 one-stage fused) and any
  * device-side wait failure (VI_ERR_TIMEOUT). */
 int vi_batch_status(vi_batch *batch, void *stream, int32_t *kernel_form);
 

@@ -88,8 +88,8 @@ def test_afda_batch_equals_unbatched(oracle_lib):
     b = ShotBatch(ws, "f32")
     b.run()
     form = b.status()
-    assert form in ("per-shot", "split")
-    variant = {"per-shot": 0, "split": 5}[form]
+    assert form in ("streams", "per-shot", "split")
+    variant = {"streams": 0, "per-shot": 0, "split": 5}[form]
     for i, w in enumerate(ws):
         tr, st = b.result(i)
         tr1, st1 = run_gpu(w, "f32", variant)

@@ -23,7 +23,7 @@ def test_batch_equals_unbatched_and_oracle(oracle_lib, kind):
     b = ShotBatch(ws, "f32")
     b.run()
     form = b.status()
-    variant = {"per-shot": 0, "split": 5, "two-stage": 3, "one-stage": 4}[form]
+    variant = {"streams": 0, "per-shot": 0, "split": 5, "two-stage": 3, "one-stage": 4}[form]
     for i, w in enumerate(ws):
         tr, st = b.result(i)
         tr1, st1 = run_gpu(w, "f32", variant)
@@ -77,8 +77,8 @@ def test_compensated_batch_matches_unbatched_and_oracle(oracle_lib, kind):
     b = ShotBatch(ws, "f32c")
     b.run()
     form = b.status()
-    assert form in ("per-shot", "split")
-    variant = {"per-shot": 0, "split": 5}[form]
+    assert form in ("streams", "per-shot", "split")
+    variant = {"streams": 0, "per-shot": 0, "split": 5}[form]
     for i, w in enumerate(ws):
         tr, st = b.result(i)
         tr1, st1 = run_gpu(w, "f32c", variant)

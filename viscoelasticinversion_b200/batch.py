@@ -59,7 +59,7 @@ class ShotBatch:
     def status(self, stream=None) -> str:
         form = C.c_int32()
         check(lib().vi_batch_status(self._h, _stream_handle(stream), C.byref(form)))
-        return {3: "per-shot", 2: "split", 1: "two-stage", 0: "one-stage", -1: "untuned"}[form.value]
+        return {4: "streams", 3: "per-shot", 2: "split", 1: "two-stage", 0: "one-stage", -1: "untuned"}[form.value]
 
     def reset(self):
         """Zeroes every shot's wavefields and traces (rest state)."""

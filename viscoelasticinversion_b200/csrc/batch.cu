@@ -23,6 +23,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fused_tma.cuh"
@@ -54,11 +55,16 @@ struct vi_batch {
   std::vector<int> prefix;
   int max_nt = 0;
   bool afda = false;  // some shot has the H-AFDA free surface
+  // concurrent per-shot form: its streams and their fork / join events
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr;
 };
 
 namespace vb {
 
-constexpr int kFormOneStage = 0, kFormTwoStage = 1, kFormSplit = 2, kFormPerShot = 3;
+constexpr int kFormOneStage = 0, kFormTwoStage = 1, kFormSplit = 2, kFormPerShot = 3, kFormStreams = 4;
+constexpr int kBatchStreams = 8;  // streams of the concurrent per-shot form
 
 static std::map<std::string, int> g_tuned;  // kernel form chosen per problem class
 static std::mutex g_tuned_mu;               // batches may run on several host threads
@@ -320,6 +326,69 @@ static int per_shot_steps(vi_batch *b, int it0, int it1, cudaStream_t st) {
   return VI_OK;
 }
 
+// The concurrent per-shot form: every shot through its own vi_step calls,
+// as in the per-shot form, spread over kBatchStreams streams so that shots
+// which do not fill the GPU run beside one another (each with the
+// single-shot kernels).  Largest work first, each shot to the stream with
+// the least work queued; one host thread per stream issues its shots, so a
+// call that waits on the host for its stream (it stages the shot's lists)
+// holds up no other stream, and the launches are issued in parallel.  The
+// streams fork from and join back into st.
+static int streams_steps(vi_batch *b, int it0, int it1, cudaStream_t st) {
+  int rc;
+  if (b->streams.empty()) {
+    b->streams.assign(kBatchStreams, nullptr);
+    b->joins.assign(kBatchStreams, nullptr);
+    for (int k = 0; k < kBatchStreams; ++k) {
+      if ((rc = cuda_check(cudaStreamCreateWithFlags(&b->streams[k], cudaStreamNonBlocking), "batch stream")))
+        return rc;
+      if ((rc = cuda_check(cudaEventCreateWithFlags(&b->joins[k], cudaEventDisableTiming), "batch event")))
+        return rc;
+    }
+    if ((rc = cuda_check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "batch event"))) return rc;
+  }
+  if ((rc = cuda_check(cudaEventRecord(b->fork, st), "fork"))) return rc;
+  for (cudaStream_t q : b->streams)
+    if ((rc = cuda_check(cudaStreamWaitEvent(q, b->fork, 0), "fork wait"))) return rc;
+  std::vector<std::pair<double, int>> work;  // (cells x steps, shot)
+  for (int i = 0; i < b->n; ++i) {
+    const int n = std::min(it1, b->nt[i]) - it0;
+    if (n > 0) work.push_back({(double)b->plans[i]->cfg.nx * b->plans[i]->cfg.nz * n, i});
+  }
+  std::stable_sort(work.begin(), work.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+  std::vector<double> load(kBatchStreams, 0.0);
+  std::vector<std::vector<int>> mine(kBatchStreams);
+  for (const auto &wk : work) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    mine[k].push_back(wk.second);
+    load[k] += wk.first;
+  }
+  std::vector<int> rcs(kBatchStreams, VI_OK);
+  std::vector<std::string> msgs(kBatchStreams);
+  std::vector<std::thread> th;
+  for (int k = 0; k < kBatchStreams; ++k) {
+    if (mine[k].empty()) continue;
+    th.emplace_back([&, k] {
+      cudaSetDevice(b->device);
+      for (int i : mine[k]) {
+        const int n = std::min(it1, b->nt[i]) - it0;
+        if ((rcs[k] = vi_step(b->plans[i], &b->med[i], &b->fields[i], &b->shot[i], it0, n, 0, b->streams[k]))) {
+          msgs[k] = vi_last_error();
+          return;
+        }
+      }
+    });
+  }
+  for (auto &t : th) t.join();
+  for (int k = 0; k < kBatchStreams; ++k)
+    if (rcs[k]) return set_error(rcs[k], msgs[k]);
+  for (int k = 0; k < kBatchStreams; ++k) {
+    if ((rc = cuda_check(cudaEventRecord(b->joins[k], b->streams[k]), "join"))) return rc;
+    if ((rc = cuda_check(cudaStreamWaitEvent(st, b->joins[k], 0), "join wait"))) return rc;
+  }
+  return VI_OK;
+}
+
 // Marginal time of 8 more steps of every shot for one form (the time of
 // 16 steps minus that of 8), so one-time costs per call — host staging of
 // the per-shot form — do not decide between forms.
@@ -363,14 +432,16 @@ static int tune(vi_batch *b, cudaStream_t st) {
   int choice = kFormTwoStage;
   // double precision has one fused form (two stages do not fit); compensated
   // FP32 and the H-AFDA surface run on the split pair only
-  const int forms[4] = {kFormPerShot, kFormSplit, kFormTwoStage, kFormOneStage};
-  const int nforms = (b->precision == VI_F32C || b->afda) ? 2 : sizeof(T) == 4 ? 4 : 3;
+  const int forms[5] = {kFormPerShot, kFormStreams, kFormSplit, kFormTwoStage, kFormOneStage};
+  const int nforms = (b->precision == VI_F32C || b->afda) ? 3 : sizeof(T) == 4 ? 5 : 4;
   for (int f = 0; f < nforms; ++f) {
     const int form = forms[f];
     float ms = 0;
     int rc;
     if (form == kFormPerShot) {
       rc = time_marginal([&](int a, int e) { return per_shot_steps(b, a, e, st); }, st, b->max_nt, &ms);
+    } else if (form == kFormStreams) {
+      rc = time_marginal([&](int a, int e) { return streams_steps(b, a, e, st); }, st, b->max_nt, &ms);
     } else {
       BatchDev<T> bd;
       rc = prepare<T>(b, form, st, bd);
@@ -419,10 +490,11 @@ static int run_impl(vi_batch *b, int flags, cudaStream_t st) {
   const int form = b->form;
   for (int i = 0; i < b->n; ++i)
     if ((rc = vi_plan_reset(b->plans[i], st))) return rc;
-  if (form == kFormPerShot) {
+  if (form == kFormPerShot || form == kFormStreams) {
     set_order(b);
     for (int i = 0; i < b->n; ++i) b->plans[i]->psi_cur = 0;
-    if ((rc = per_shot_steps(b, 0, b->max_nt, st))) return rc;
+    if ((rc = form == kFormStreams ? streams_steps(b, 0, b->max_nt, st) : per_shot_steps(b, 0, b->max_nt, st)))
+      return rc;
     return cuda_check(cudaGetLastError(), "batch run");
   }
   if (b->dirty || !use_graph || b->graph_form != form) {
@@ -544,6 +616,11 @@ extern "C" int vi_batch_destroy(vi_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->dev) cudaFree(b->dev);
   if (b->err) cudaFree(b->err);
+  for (cudaStream_t q : b->streams)
+    if (q) cudaStreamDestroy(q);
+  for (cudaEvent_t e : b->joins)
+    if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
   for (vi_plan *p : b->plans) vi_plan_destroy(p);
   delete b;
   return VI_OK;
@@ -590,7 +667,7 @@ extern "C" int vi_batch_status(vi_batch *b, void *stream, int32_t *kernel_form) 
   int flag = 0;
   rc = cuda_check(cudaMemcpy(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
   if (rc) return rc;
-  // the per-shot form reports through each shot's plan
+  // the per-shot forms report through each shot's plan
   for (int i = 0; i < b->n; ++i) {
     int pf = 0;
     if ((rc = cuda_check(cudaMemcpy(&pf, b->plans[i]->errflag, sizeof(int), cudaMemcpyDeviceToHost),
