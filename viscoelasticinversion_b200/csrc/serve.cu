@@ -104,6 +104,7 @@ struct Req {
   bool busy = false;          // a lane is advancing it (under the server lock)
   uint64_t last_turn = 0;     // round robin: when it last got a slice
   std::shared_ptr<GradRun> gr;  // gradient requests, once started
+  bool started = false;         // has had a slice (under the server lock)
 };
 
 size_t esize_of(const vi_config &c) { return c.precision == VI_F64 ? 8 : 4; }
@@ -404,17 +405,22 @@ bool can_admit(const vi_server *s) {
 // run gradients an idle forward request goes first: the forward stream is
 // never left without a lane
 std::shared_ptr<Req> pick_idle(vi_server *s) {
-  int grads = 0;
+  int grads = 0, open_grads = 0;
   bool idle_fwd = false;
   for (auto &q : s->active) {
     if (q->busy && q->rq.kind == VI_REQ_GRADIENT) ++grads;
+    if (q->started && q->rq.kind == VI_REQ_GRADIENT) ++open_grads;
     if (!q->busy && q->rq.kind != VI_REQ_GRADIENT) idle_fwd = true;
   }
   const bool hold_grads = s->cfg.lanes > 1 && grads >= s->cfg.lanes - 1 && idle_fwd;
+  // at most `lanes` gradients in progress at once, as when each ran whole:
+  // a started gradient holds its checkpoint workspace until it ends
+  const bool hold_new_grads = open_grads >= s->cfg.lanes;
   std::shared_ptr<Req> best;
   for (auto &q : s->active) {
     if (q->busy) continue;
     if (hold_grads && q->rq.kind == VI_REQ_GRADIENT) continue;
+    if (hold_new_grads && !q->started && q->rq.kind == VI_REQ_GRADIENT) continue;
     if (!best) {
       best = q;
     } else if (s->cfg.policy == VI_SERVE_ROUND_ROBIN ? q->last_turn < best->last_turn
@@ -423,12 +429,6 @@ std::shared_ptr<Req> pick_idle(vi_server *s) {
     }
   }
   return best;
-}
-
-bool any_idle(const vi_server *s) {
-  for (auto &q : s->active)
-    if (!q->busy) return true;
-  return false;
 }
 
 void lane_main(vi_server *s) {
@@ -440,7 +440,7 @@ void lane_main(vi_server *s) {
       const auto drained = [&] {
         return s->stopping && s->queue.empty() && s->active.empty() && s->admitting == 0;
       };
-      s->cv.wait(lk, [&] { return can_admit(s) || any_idle(s) || drained(); });
+      s->cv.wait(lk, [&] { return can_admit(s) || pick_idle(s) != nullptr || drained(); });
       if (can_admit(s)) {
         adm = s->queue.front();
         s->queue.pop_front();
@@ -449,6 +449,7 @@ void lane_main(vi_server *s) {
         ++s->admitting;
       } else if ((pick = pick_idle(s))) {
         pick->busy = true;
+        pick->started = true;
         pick->last_turn = ++s->turn;
       } else {
         return;  // drained
