@@ -1,17 +1,22 @@
 #!/usr/bin/env python
-"""Benchmark of the fused viscoelastic time step (one JSON line on rank 0).
+"""Benchmark of the viscoelastic time step (one JSON line on rank 0).
 
 A bench "step" is one whole forward solve of the single-shot workload:
 2048 x 1024 grid, dx = 5 m, dt = 0.4 ms, 4000 time steps, FP32, seeded
 8-layer VTI medium with 3 SLS mechanisms, 40-cell CPML, free surface,
-12 Hz explosive Ricker and 512 receivers (synthetic inputs).
+12 Hz explosive Ricker and 512 receivers (synthetic inputs), on the
+default kernel path (the split velocity/stress pair).
 
   value  Gpt/s = nx*nz*nt / time, inputs resident in HBM, max over ranks,
          summed over ranks (one independent shot per GPU: weak scaling)
   e2e    the same through vi_forward_host with pinned host buffers: medium
          and wavelet upload, the solve, and the trace download per step
-  roofline  algorithmic bytes per fused launch / mean launch time vs the
-         measured HBM copy bandwidth
+  roofline  algorithmic bytes per time step (one velocity + one stress
+         launch) / mean step time vs the measured HBM copy bandwidth
+  accuracy  the timed solve against the same solve in FP64 (untimed)
+  batched, batched_small  64-shot TTI gathers, batched vs one at a time
+  gradient  the 16-shot 1024 x 512 FWI gradient, with FD and FP32 checks
+  serving  the mixed request stream, continuous vs FIFO
   cpu_baseline  the CPU oracle (FP32 twin, all host threads) on a bounded
          sample of the same workload (rank 0, N = 1)
 
