@@ -134,7 +134,7 @@ def measured_peaks():
 
 KERNEL_NAMES = {"fused-tma": "k_fused_tma", "fused-tma-1stage": "k_fused_tma", "fused": "k_fused",
                 "plain": "k_plain", "split": "k_split", "split-pipelined": "k_split_p",
-                "split-ldg": "k_split", "stream": "k_stream"}
+                "split-ldg": "k_split", "stream": "k_stream", "wave": "k_wave"}
 KERNEL_PAIRS = {"split": "k_split_vel_tma + k_split_stress",
                 "split-ldg": "k_split_vel_ldg + k_split_stress",
                 "split-pipelined": "k_split_vel_p + k_split_stress_p"}
@@ -144,14 +144,16 @@ def kernels_per_step(kernel: str, w) -> int:
     """Kernels of this library launched per time step by each path."""
     if kernel.startswith("split"):
         return 2
+    if kernel == "wave":  # one persistent launch per solve, not per step
+        return 0
     if kernel == "plain":  # velocity, strain, update (+ surface rate, mirror, sources, receivers)
         return 3 + (2 if w.free_surface else 0) + (2 if w.sources else 0) + (1 if w.receivers else 0)
     return 1
 
 
 def ncu_traffic(name: str):
-    """DRAM bytes per launch of the fused kernel from the committed ncu
-    summary of this workload (profiles/), or None."""
+    """DRAM bytes per time step of the default kernel pair from the
+    committed ncu summary of this workload (profiles/), or None."""
     f = ROOT / "profiles" / f"{name}.ncu.md"
     if not f.exists():
         return None
@@ -652,7 +654,7 @@ def run_ours(a):
     peak, peak_kind = measured_peaks()
     kernel = plan.last_kernel()
     kname = KERNEL_NAMES.get(kernel, kernel)
-    kernels = kernels_per_step(kernel, w) * w.nt
+    kernels = kernels_per_step(kernel, w) * w.nt or 1  # the time-blocked form: one launch per solve
     traffic = ncu_traffic(f"{kname}_{w.kind}_{w.nx}x{w.nz}")
 
     out = {
